@@ -1,0 +1,31 @@
+"""ctypes signatures of include/compact_b200.h."""
+import ctypes
+
+vp = ctypes.c_void_p
+i32 = ctypes.c_int
+u32 = ctypes.c_uint
+f64 = ctypes.c_double
+sz = ctypes.c_size_t
+
+
+def declare(L):
+    from . import Dcomp
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    L.cs_last_error.restype = ctypes.c_char_p
+    L.cs_version.restype = i32
+    L.cs_numerics_create.argtypes = [pp, Dcomp, vp]
+    L.cs_numerics_destroy.argtypes = [vp]
+    L.cs_deriv_setup.argtypes = [vp]
+    L.cs_get_coeffs.argtypes = [vp, vp, vp]
+    L.cs_get_ndf.argtypes = [vp, vp]
+    L.cs_get_buffers.argtypes = [vp, i32, pp, pp, pp]
+    L.cs_deriv.argtypes = [vp, i32, vp, vp, i32, i32, Dcomp, u32, u32, u32, i32, vp]
+    L.cs_deriv_f32.argtypes = [vp, i32, vp, vp, i32, i32, Dcomp, u32, u32, u32, i32, vp]
+    L.cs_fill_buffers.argtypes = [vp, vp, i32, i32, i32, Dcomp, vp]
+    L.cs_halo_exchange_self.argtypes = [vp, u32, vp]
+    L.cs_filter.argtypes = [vp, i32, vp, vp, f64, Dcomp, vp]
+    L.cs_line_tables.argtypes = [i32, i32, i32, i32, f64, vp, vp, sz]
+    for name in ("cs_numerics_create", "cs_numerics_destroy", "cs_deriv_setup", "cs_get_coeffs",
+                 "cs_get_ndf", "cs_get_buffers", "cs_deriv", "cs_deriv_f32", "cs_fill_buffers",
+                 "cs_halo_exchange_self", "cs_filter", "cs_line_tables"):
+        getattr(L, name).restype = i32

@@ -1,0 +1,274 @@
+// line_solver.cuh -- device side of the compact_schemes_b200 line solver.
+//
+// One warp solves one line of n <= 1024 points.  Lane c owns the contiguous
+// chunk of rows [c*LT, c*LT + len) in registers.  The solve is the
+// partitioned ("modified Thomas" + PCR) algorithm:
+//   1. each lane eliminates inside its chunk (forward then backward sweep),
+//      leaving its first and last rows coupled only to the neighbouring
+//      chunks' end rows;
+//   2. the 64-row reduced system (2 rows per lane) is solved by six
+//      parallel-cyclic-reduction steps over warp shuffles;
+//   3. each lane back-substitutes its interior rows.
+// Because every line of one configuration shares its matrix, all elimination
+// factors are precomputed on the host (tables.cpp); the device work per row
+// is a handful of FMAs on the right-hand side only.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "cs_common.h"
+
+namespace csb {
+
+template <typename CT>
+struct DevTables {
+    const CT *fwd1, *fwd2, *bwd1, *bwd2, *rca, *rcc, *k1, *k2, *invb, *cycz;
+    CT cyc_s1, cyc_s2;
+    int n, p, last_len, cyclic;
+};
+
+// Shared-memory layout of one line: element j = c*LT + t lives at
+// t*32 + ((c + (32/LT)*t) & 31).  Lane c reading its element t touches 32
+// consecutive words (conflict free); 32 threads writing consecutive j also
+// spread over all banks.
+template <int LT>
+struct LineLayout {
+    static constexpr int kRot = 32 / LT;
+    static constexpr int kSlot = 32 * LT + 1;  // odd stride between lines of a tile
+    __device__ __forceinline__ static int pos(int j) {
+        const int c = j / LT, t = j % LT;
+        return t * 32 + ((c + kRot * t) & 31);
+    }
+    __device__ __forceinline__ static int pos_ct(int c, int t) { return t * 32 + ((c + kRot * t) & 31); }
+};
+
+__device__ __forceinline__ int lane_len(int lane, int lt, int p, int last_len) {
+    return lane < p - 1 ? lt : (lane == p - 1 ? last_len : 0);
+}
+
+// Solve NV right-hand sides held as d[v][t] by the lanes of one warp; the
+// solution overwrites d.  All 32 lanes must call it (warp shuffles).
+template <int LT, int NV, typename CT>
+__device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][LT], int lane) {
+    const int len = lane_len(lane, LT, T.p, T.last_len);
+#pragma unroll
+    for (int t = 0; t < LT; ++t) {
+        const CT f1 = T.fwd1[t * 32 + lane];
+        if (t == 0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) d[v][0] = f1 * d[v][0];
+        } else {
+            const CT f2 = T.fwd2[t * 32 + lane];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) d[v][t] = f1 * d[v][t] + f2 * d[v][t - 1];
+        }
+    }
+#pragma unroll
+    for (int t = LT - 2; t >= 0; --t) {
+        const CT b1 = T.bwd1[t * 32 + lane], b2 = T.bwd2[t * 32 + lane];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) d[v][t] = b1 * d[v][t] + b2 * d[v][t + 1];
+    }
+    CT y0[NV], y1[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        y0[v] = d[v][0];
+        y1[v] = CT(0);
+#pragma unroll
+        for (int t = 1; t < LT; ++t)
+            if (t == len - 1) y1[v] = d[v][t];
+    }
+    {
+        const CT ka = T.k1[lane], kb = T.k2[lane], kc = T.k1[32 + lane], kd = T.k2[32 + lane];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const CT up1 = __shfl_up_sync(0xffffffffu, y1[v], 1);
+            const CT dn0 = __shfl_down_sync(0xffffffffu, y0[v], 1);
+            const CT n0 = y0[v] - ka * up1 - kb * y1[v];
+            const CT n1 = y1[v] - kc * y0[v] - kd * dn0;
+            y0[v] = n0;
+            y1[v] = n1;
+        }
+    }
+#pragma unroll
+    for (int s = 1; s < kPcrSteps; ++s) {
+        const int dl = 1 << (s - 1);
+        const CT ka = T.k1[s * 64 + lane], kb = T.k2[s * 64 + lane];
+        const CT kc = T.k1[s * 64 + 32 + lane], kd = T.k2[s * 64 + 32 + lane];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const CT u0 = __shfl_up_sync(0xffffffffu, y0[v], dl);
+            const CT d0 = __shfl_down_sync(0xffffffffu, y0[v], dl);
+            const CT u1 = __shfl_up_sync(0xffffffffu, y1[v], dl);
+            const CT d1 = __shfl_down_sync(0xffffffffu, y1[v], dl);
+            y0[v] = y0[v] - ka * u0 - kb * d0;
+            y1[v] = y1[v] - kc * u1 - kd * d1;
+        }
+    }
+    const CT ib0 = T.invb[lane], ib1 = T.invb[32 + lane];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const CT X0 = y0[v] * ib0, X1 = y1[v] * ib1;
+#pragma unroll
+        for (int t = 0; t < LT; ++t) {
+            CT x = d[v][t] - T.rca[t * 32 + lane] * X0 - T.rcc[t * 32 + lane] * X1;
+            if (t == 0) x = X0;
+            if (t != 0 && t == len - 1) x = X1;
+            d[v][t] = x;
+        }
+        if (T.cyclic) {
+            const CT last = len >= 2 ? X1 : X0;
+            const CT ya = __shfl_sync(0xffffffffu, X0, 0);
+            const CT yb = __shfl_sync(0xffffffffu, last, T.p - 1);
+            const CT beta = (ya + T.cyc_s2 * yb) * T.cyc_s1;
+#pragma unroll
+            for (int t = 0; t < LT; ++t) d[v][t] -= beta * T.cycz[t * 32 + lane];
+        }
+    }
+}
+
+// Select d[t] for a runtime t without dynamic register indexing.
+template <int LT, typename CT>
+__device__ __forceinline__ void set_at(CT (&d)[LT], int t, CT val) {
+#pragma unroll
+    for (int k = 0; k < LT; ++k)
+        if (k == t) d[k] = val;
+}
+template <int LT, typename CT>
+__device__ __forceinline__ CT get_at(const CT (&d)[LT], int t) {
+    CT r = CT(0);
+#pragma unroll
+    for (int k = 0; k < LT; ++k)
+        if (k == t) r = d[k];
+    return r;
+}
+
+// Right-hand side of the compact derivative for the rows of this lane,
+// restating build_system (src/cuda/kernels/numerics_device_pc.hpp:176-293):
+// interior aa*(f[j+1]-f[j-1]) + bb*(f[j+2]-f[j-2]); physical closure rows
+// (ndf = 0) or interface closure rows (ndf = 1: 8-point pbci sums plus the
+// received pbco sums; `recv4` = {row0, row1, row n-1, row n-2} received
+// values, or the line's own far-end sums for single-rank periodic).
+// `f` is the line in LineLayout<LT> order in shared memory.
+template <int LT, typename CT, typename FT>
+__device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nstart, int nend,
+                                          const CT *recv4_or_null, const Coeffs &cf,
+                                          CT (&d)[LT]) {
+    using L = LineLayout<LT>;
+    const int j0 = lane * LT;
+    CT w[LT + 4];
+#pragma unroll
+    for (int k = 0; k < LT + 4; ++k) {
+        int j = j0 + k - 2;
+        j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
+        w[k] = CT(f[L::pos(j)]);
+    }
+#pragma unroll
+    for (int t = 0; t < LT; ++t)
+        d[t] = (j0 + t < n) ? CT(kAa) * (w[t + 3] - w[t + 1]) + CT(kBb) * (w[t + 4] - w[t]) : CT(0);
+
+    const bool own_lo = lane == 0;
+    const int own_hi1 = (n - 1) / LT, own_hi2 = (n - 2) / LT;
+    if (own_lo || lane == own_hi1 || lane == own_hi2) {
+        // the few boundary rows are rebuilt from scratch by their owner lanes
+        if (own_lo) {
+            const CT f0 = CT(f[L::pos(0)]), f1 = CT(f[L::pos(1)]), f2 = CT(f[L::pos(2)]);
+            if (nstart == 0) {
+                d[0] = CT(kAb00) * f0 + CT(kAb01) * f1 + CT(kAb02) * f2;
+                d[1] = CT(kAb10) * (f2 - f0);
+            } else {
+                CT r0, r1;
+                if (recv4_or_null) {
+                    r0 = recv4_or_null[0];
+                    r1 = recv4_or_null[1];
+                } else {
+                    r0 = CT(0);
+                    r1 = CT(0);
+#pragma unroll
+                    for (int k = 0; k < kLmd; ++k) r0 += CT(cf.pbco[k]) * CT(f[L::pos(n - 1 - k)]);
+#pragma unroll
+                    for (int k = 0; k < kLmd; ++k) r1 += CT(cf.pbco[kLmd + k]) * CT(f[L::pos(n - 1 - k)]);
+                }
+                CT s0 = CT(0), s1 = CT(0);
+#pragma unroll
+                for (int k = 0; k < kLmd; ++k) s0 += CT(cf.pbci[k]) * CT(f[L::pos(k)]);
+#pragma unroll
+                for (int k = 0; k < kLmd; ++k) s1 += CT(cf.pbci[kLmd + k]) * CT(f[L::pos(k)]);
+                d[0] = s0 + r0;
+                d[1] = s1 + r1;
+            }
+        }
+        if (lane == own_hi1 || lane == own_hi2) {
+            const CT g0 = CT(f[L::pos(n - 1)]), g1 = CT(f[L::pos(n - 2)]), g2 = CT(f[L::pos(n - 3)]);
+            CT e1, e2;  // rows n-1 and n-2
+            if (nend == 0) {
+                e1 = -(CT(kAb00) * g0 + CT(kAb01) * g1 + CT(kAb02) * g2);
+                e2 = -CT(kAb10) * (g2 - g0);
+            } else {
+                CT r2, r3;
+                if (recv4_or_null) {
+                    r2 = recv4_or_null[2];
+                    r3 = recv4_or_null[3];
+                } else {
+                    r2 = CT(0);
+                    r3 = CT(0);
+#pragma unroll
+                    for (int k = 0; k < kLmd; ++k) r2 += CT(cf.pbco[k]) * CT(f[L::pos(k)]);
+#pragma unroll
+                    for (int k = 0; k < kLmd; ++k) r3 += CT(cf.pbco[kLmd + k]) * CT(f[L::pos(k)]);
+                }
+                CT s0 = CT(0), s1 = CT(0);
+#pragma unroll
+                for (int k = 0; k < kLmd; ++k) s0 += CT(cf.pbci[k]) * CT(f[L::pos(n - 1 - k)]);
+                s0 += r2;
+#pragma unroll
+                for (int k = 0; k < kLmd; ++k) s1 += CT(cf.pbci[kLmd + k]) * CT(f[L::pos(n - 1 - k)]);
+                s1 += r3;
+                e1 = -s0;
+                e2 = -s1;
+            }
+            if (lane == own_hi1) set_at<LT, CT>(d, (n - 1) - lane * LT, e1);
+            if (lane == own_hi2) set_at<LT, CT>(d, (n - 2) - lane * LT, e2);
+        }
+    }
+}
+
+// Right-hand side of the sixth-order tridiagonal filter (Gaitonde & Visbal):
+//   sum_m a_m/2 (f[j+m] + f[j-m]); near non-periodic ends the boundary point
+// is copied and points 1 / 2 use the second / fourth order centred formulas.
+// cyclic: indices wrap.
+template <int LT, typename CT, typename FT>
+__device__ __forceinline__ void filter_rhs(const FT *f, int n, int lane, bool cyclic, CT af,
+                                           CT (&d)[LT]) {
+    using L = LineLayout<LT>;
+    const CT a60 = (CT(11) + CT(10) * af) / CT(16), a61 = (CT(15) + CT(34) * af) / CT(32);
+    const CT a62 = (CT(-3) + CT(6) * af) / CT(16), a63 = (CT(1) - CT(2) * af) / CT(32);
+    const CT a40 = (CT(5) + CT(6) * af) / CT(8), a41 = (CT(1) + CT(2) * af) / CT(2);
+    const CT a42 = (CT(-1) + CT(2) * af) / CT(8);
+    const CT a20 = (CT(1) + CT(2) * af) / CT(2);
+    const int j0 = lane * LT;
+    CT w[LT + 6];
+#pragma unroll
+    for (int k = 0; k < LT + 6; ++k) {
+        int j = j0 + k - 3;
+        if (cyclic) j = j < 0 ? j + n : (j >= n ? j - n : j);
+        else j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
+        w[k] = CT(f[L::pos(j)]);
+    }
+#pragma unroll
+    for (int t = 0; t < LT; ++t) {
+        const int j = j0 + t;
+        const CT c0 = w[t + 3];
+        const CT s1 = w[t + 4] + w[t + 2], s2 = w[t + 5] + w[t + 1], s3 = w[t + 6] + w[t];
+        CT r = a60 * c0 + CT(0.5) * (a61 * s1 + a62 * s2 + a63 * s3);
+        if (!cyclic) {
+            const int dist = j < n - 1 - j ? j : n - 1 - j;
+            if (dist == 0) r = c0;
+            else if (dist == 1) r = a20 * c0 + CT(0.5) * a20 * s1;
+            else if (dist == 2) r = a40 * c0 + CT(0.5) * (a41 * s1 + a42 * s2);
+        }
+        d[t] = j < n ? r : CT(0);
+    }
+}
+
+}  // namespace csb

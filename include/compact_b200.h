@@ -1,0 +1,123 @@
+/*
+ * compact_b200.h -- C ABI of compact_schemes_b200, a B200 (sm_100a)
+ * implementation of the compact-scheme hot path of EnricoDeg/compact_schemes.
+ *
+ * Conventions
+ *  - Fields are structure-of-arrays in device memory, q[v*lmx + idx] with
+ *    idx = i + lxi*(j + let*k) (x fastest), exactly the reference layout
+ *    (src/cuda/kernels/physics.hpp:55-100).  All pointers passed to compute
+ *    entry points are device pointers unless the name says _host.
+ *  - Every entry point returns an int status (CS_OK = 0, negative on error)
+ *    instead of the reference's print-and-exit (src/cuda/check.hpp:36-41);
+ *    cs_last_error() gives a message.
+ *  - `stream` is a cudaStream_t passed as void*; 0 = legacy default stream.
+ *    No entry point synchronizes the host unless documented.
+ *  - The whole domain is one rank: the reference's MPI halo exchange
+ *    (numerics_base::mpigo, src/numerics_base.hpp:119-180) becomes a local
+ *    copy for faces whose neighbour is the block itself (periodic).
+ *
+ * Each declaration cites the reference interface it replaces (file:line,
+ * relative to the reference project root).
+ */
+#ifndef COMPACT_B200_H
+#define COMPACT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CS_OK 0
+#define CS_ERR_INVALID (-1)     /* bad argument (dims, pointer, axis, size) */
+#define CS_ERR_CUDA (-2)        /* CUDA runtime error */
+#define CS_ERR_UNSUPPORTED (-3) /* line too long/short for the kernels */
+#define CS_ERR_ALLOC (-4)       /* device allocation failed */
+#define CS_ERR_STATE (-5)       /* call order (e.g. deriv before deriv_setup) */
+
+/* Boundary codes, src/common/parameters.hpp:46-52. */
+#define CS_BC_NON_REFLECTIVE 10
+#define CS_BC_WALL_INVISCID 20
+#define CS_BC_WALL_VISCOUS 25
+#define CS_BC_INTER_CURV 30
+#define CS_BC_INTER_STRAIGHT 35
+#define CS_BC_INTER_SUBDOMAINS 40
+#define CS_BC_PERIODIC 45
+
+/* Halo source for interface (ndf = 1) faces of a derivative. */
+#define CS_HALO_RECV 0 /* read the numerics object's recv buffer (reference data flow) */
+#define CS_HALO_SELF 1 /* single-rank periodic: sums taken in-kernel from the line's far end */
+
+/* t_dcomp, src/common/data_types.hpp:33-39 (point counts). */
+typedef struct {
+    int lmx;
+    int lxi;
+    int let;
+    int lze;
+} cs_dcomp;
+
+const char *cs_last_error(void);
+int cs_version(void);
+
+/* ---------------------------------------------------------------------------
+ * numerics: compact derivative / filter line solves
+ * ------------------------------------------------------------------------- */
+typedef struct cs_numerics cs_numerics;
+
+/* numerics_base<T>(t_dcomp, int nbc[2][3]) (src/numerics_base.hpp:43-93):
+ * allocates drva/send/recv scratch per axis and derives ndf per face. */
+int cs_numerics_create(cs_numerics **out, cs_dcomp d, const int nbc[2][3]);
+/* ~numerics_base (src/numerics_base.hpp:96-112). */
+int cs_numerics_destroy(cs_numerics *nm);
+/* numerics_base::deriv_setup (src/numerics_base.hpp:182-297): interface
+ * weights pbco/pbci (copied to the device) and the line-solver tables. */
+int cs_deriv_setup(cs_numerics *nm);
+/* Host copies of pbco/pbci (16 each). */
+int cs_get_coeffs(const cs_numerics *nm, double pbco[16], double pbci[16]);
+/* ndf[face][axis] as in numerics_base::ndf (src/numerics_base.hpp:73-93). */
+int cs_get_ndf(const cs_numerics *nm, int ndf[2][3]);
+/* Device scratch owned by the object (numerics_base::drva_buffer,
+ * send_buffer, recv_buffer, src/numerics_base.hpp:389-395):
+ * drva [2][5][F], send/recv [5][2][2][F] for the given axis (F = face size). */
+int cs_get_buffers(cs_numerics *nm, int axis, double **drva, double **send, double **recv);
+
+/* numerics_pc::deriv1d / deriv2d (src/numerics_pc.hpp:74-168): compact first
+ * derivative along `axis` in index space of in[comp*lmx + .] into
+ * out[slot*lmx + .] (deriv1d: comp = slot = 0; deriv2d: slot = axis).
+ * nstart/nend: ndf of face 0 / 1.  Line-end values go to drva[axis] at
+ * variable `var`.  halo: CS_HALO_RECV or CS_HALO_SELF.  FP64. */
+int cs_deriv(cs_numerics *nm, int axis, const double *in, double *out, int nstart, int nend,
+             cs_dcomp d, unsigned var, unsigned comp, unsigned slot, int halo, void *stream);
+/* Same for numerics_pc<float>: FP32 data and arithmetic. */
+int cs_deriv_f32(cs_numerics *nm, int axis, const float *in, float *out, int nstart, int nend,
+                 cs_dcomp d, unsigned var, unsigned comp, unsigned slot, int halo, void *stream);
+
+/* numerics_pc::fill_buffers<m0,m1> (src/numerics_pc.hpp:231-287) with
+ * gpu_buffer::fill / fill_gpu_buffer_kernel (src/cuda/kernels/numerics_pc.hpp:42-122):
+ * pbco-weighted interface sums of variables [var_lo, var_hi) of the
+ * [5][3][lmx] field block `in` into the send buffers.  nrt as the reference. */
+int cs_fill_buffers(cs_numerics *nm, const double *in, int var_lo, int var_hi, int nrt,
+                    cs_dcomp d, void *stream);
+/* Single-rank numerics_base::mpigo (src/numerics_base.hpp:119-180): for every
+ * axis whose two faces are interface faces (ndf = 1) the block is its own
+ * neighbour; recv of face 0 <- send of face 1 and vice versa, variable var. */
+int cs_halo_exchange_self(cs_numerics *nm, unsigned var, void *stream);
+
+/* Compact filter along `axis` (no reference implementation: the sixth-order
+ * tridiagonal filter of Gaitonde & Visbal).  ndf faces of the
+ * axis both 1: cyclic; both 0: reduced-order boundary closure. */
+int cs_filter(cs_numerics *nm, int axis, const double *in, double *out, double alpha_f,
+              cs_dcomp d, void *stream);
+
+/* Introspection of the line-solver tables (tests, autotuner): fills meta =
+ * {n, lt, p, last_len, cyclic} and, if tables != NULL, the 6*lt*32 + 13*64 +
+ * lt*32 doubles fwd1,fwd2,bwd1,bwd2,rca,rcc,k1,k2,invb,cycz,{s1,s2}.
+ * scheme 0 = derivative (nstart/nend), 1 = filter (alpha_f). */
+int cs_line_tables(int n, int scheme, int nstart, int nend, double alpha_f, int meta[5],
+                   double *tables, size_t tables_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
