@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Headline benchmark: plain FP64 compressible Navier-Stokes RHS + RK stage update
+on a 256^3 periodic Taylor-Green box (Mach 0.1, Re 1600, gamma 1.4, Pr 0.71,
+1e-4 seeded density noise, CFL 0.5 with dt recomputed on the device every step).
+
+A step is one RK step = 4 RK stages over the whole box.  Throughput is
+grid-point RK-stage updates per second (Mpts*RK-stages/s), whole job.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Timed regions (all on the device with CUDA events, barrier + synchronize on
+both sides, max over ranks):
+  value     K graph-replayed steps on a device-resident state;
+  roofline  K eager steps with CUDA events around every pass (same workload);
+  e2e       K steps through cs_solver_step_host: pinned host state -> device,
+            step, device -> host, every step.
+The state (5 x 134 MB) and the gradient scratch (12 x 134 MB) are far larger
+than the 126 MB L2, so no flush is needed between steps.
+With --gpus N > 1 every rank advances its own independent 256^3 box (replicas,
+weak scaling; the only collective is the timing max).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpts*RK-stages/s at 256^3: mixed vs plain FP64 at <=1e-6 rel err; adjoint/fwd time"
+UNIT = "Mpts*RK-stages/s"
+MACH, RE, CFL = 0.1, 1600.0, 0.5
+# Algorithmic bytes per grid point per launch of each pass (FP64, constant
+# metrics): gradient pass reads q (5) and writes 4 gradients; flux x reads q
+# and 12 gradients and writes R; flux y also reads R; flux z + RK reads q,
+# 12 gradients, R and q^n and writes q (stage 0: q^n is the stage input).
+ALG_BYTES = {"grad_x": 72, "grad_y": 72, "grad_z": 72, "flux_x": 176, "flux_y": 216,
+             "flux_z_rk": 8 * (5 + 12 + 5 + 5 + 5)}
+STAGE_BYTES = 864  # sum of the passes above per point per stage
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=256)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f:
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                smax.append(float(c[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def cpu_oracle_stage_rate(n, stages=1):
+    """Oracle (FP64 C++/OpenMP restatement) RK stages at n^3 on the host cores."""
+    import numpy as np
+    import oracle as O
+    dims = (n, n, n)
+    q = O.tgv_init(dims, MACH, 1e-4, 0)
+    q1 = np.empty_like(q)
+    m = O.uniform_metrics(*dims)
+    nbc = [[45] * 3, [45] * 3]
+    de, _ = O.thermo(q)
+    dt = O.time_step_m(de, m, MACH / RE, (0.0, 0.0, 0.0), CFL)
+    del de
+    t0 = time.perf_counter()
+    for k in range(stages):
+        O.rk_stage(q, q if k == 0 else q1, q1, k % 4, dt, MACH / RE, m, dims, nbc)
+    t = time.perf_counter() - t0
+    return n ** 3 * stages / t / 1e6, t, O.num_threads()
+
+
+def run_reference(args):
+    """Reference arm: the reference has no CPU implementation of the path, so its
+    CPU path is the oracle port of its kernels, timed on the host cores."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np
+    import oracle as O
+    n = args.n
+    dims = (n, n, n)
+    q = O.tgv_init(dims, MACH, 1e-4, 0)
+    q1 = np.empty_like(q)
+    m = O.uniform_metrics(*dims)
+    nbc = [[45] * 3, [45] * 3]
+    de, _ = O.thermo(q)
+    dt = O.time_step_m(de, m, MACH / RE, (0.0, 0.0, 0.0), CFL)
+    del de
+    for k in range(args.warmup):
+        O.rk_stage(q, q if k == 0 else q1, q1, k % 4, dt, MACH / RE, m, dims, nbc)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        O.rk_stage(q, q1, q1, (k + 1) % 4, dt, MACH / RE, m, dims, nbc)
+    t = time.perf_counter() - t0
+    value = n ** 3 * args.steps / t / 1e6
+    cores = O.num_threads()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "taylor_green_256^3_fp64_plain", "n": n, "step": "one RK stage",
+                       "mach": MACH, "re": RE, "cfl": CFL},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d RK stages of the %d^3 Taylor-Green box (FP64 oracle, "
+                                       "C++/OpenMP restatement of the reference kernels)" % (args.steps, n)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import compact_schemes_b200 as cs
+
+    world, rank, local = dist_setup(args)
+    n = args.n
+    dims = (n, n, n)
+    lmx = n ** 3
+    pts_stages_per_step = lmx * 4
+    cfg = cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True)
+    s = cs.Solver(cfg)
+    q = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
+    cs.tgv_init(q, dims, MACH, 1e-4, rank)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        s.step(q, 0.0)
+    barrier(world)
+
+    # --- value: graph-replayed steps on the device-resident state -------------
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.step(q, 0.0)
+    e1.record(stream)
+    barrier(world)
+    clocks = clk.stop()
+    t_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    value = world * pts_stages_per_step * args.steps / (t_ms * 1e-3) / 1e6
+
+    # --- roofline: eager steps with per-pass events ------------------------------
+    s.profile_begin()
+    for _ in range(args.steps):
+        s.step(q, 0.0)
+    prof = s.profile_end()
+    barrier(world)
+    hbm, peak_kind = peaks()
+    per_pass = {}
+    for k, (ms, cnt) in prof.items():
+        if cnt:
+            per_pass[k] = {"ms_per_launch": ms / cnt, "launches": cnt, "total_ms": ms}
+    top = max(per_pass, key=lambda k: per_pass[k]["total_ms"])
+    alg = ALG_BYTES[top] * lmx
+    if top == "flux_z_rk":  # stage 0 reads q^n only once
+        alg = (3 * ALG_BYTES[top] + (ALG_BYTES[top] - 40)) / 4 * lmx
+    achieved = alg / (per_pass[top]["ms_per_launch"] * 1e-3) / 1e9
+    stage_ms = sum(v["total_ms"] for v in per_pass.values()) / (4 * args.steps)
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        if top in tj:
+            traffic = tj[top]["bytes_per_point"] * lmx
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic, "kernel": top,
+                "peak_source": peak_kind,
+                "alg_bytes_per_launch": alg}
+
+    # --- e2e: host buffers through cs_solver_step_host ------------------------------
+    qh_in = torch.empty(5 * lmx, dtype=torch.float64, pin_memory=True)
+    qh_out = torch.empty(5 * lmx, dtype=torch.float64, pin_memory=True)
+    qh_in.copy_(q.cpu())
+    s.step_host(qh_in, qh_out, 0.0)  # first call allocates the solver-owned state
+    barrier(world)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        s.step_host(qh_in, qh_out, 0.0)
+        qh_in, qh_out = qh_out, qh_in
+    f1.record(stream)
+    barrier(world)
+    te_ms = max_over_ranks(f0.elapsed_time(f1), world)
+    e2e = {"value": world * pts_stages_per_step * args.steps / (te_ms * 1e-3) / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": 5 * lmx * 8, "d2h_bytes_per_step": 5 * lmx * 8,
+           "ms_per_step": te_ms / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, t, cores = cpu_oracle_stage_rate(n, stages=1)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "1 RK stage of the %d^3 Taylor-Green box in %.1f s (FP64 oracle, "
+                         "C++/OpenMP restatement of the reference kernels)" % (n, t)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": "taylor_green_256^3_fp64_plain" if n == 256 else
+                           "taylor_green_%d^3_fp64_plain" % n,
+                           "n": n, "mach": MACH, "re": RE, "cfl": CFL, "dt": "CFL, every step, on device",
+                           "rk": "4-stage, q^(k) = q^n - dt/(4-k) J R", "bc": "periodic (quasi-disjoint closure)",
+                           "l2": "inputs larger than L2 (state 671 MB + gradients 1.6 GB), no flush",
+                           "parallelism": "replicas" if world > 1 else "single GPU"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 24 * args.steps, "clocks": clocks,
+                "passes": per_pass,
+                "stage_model": {"bytes_per_point": STAGE_BYTES, "ms_per_stage": stage_ms,
+                                "achieved_gbs": STAGE_BYTES * lmx / (stage_ms * 1e-3) / 1e9,
+                                "frac": STAGE_BYTES * lmx / (stage_ms * 1e-3) / 1e9 / hbm}}
+        print(json.dumps(line))
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -87,3 +87,4 @@ def nbc_array(nbc):
 
 
 from .numerics import numerics_pc, numerics_rtc  # noqa: E402,F401
+from .solver import Solver, SolverConfig, tgv_config, tgv_init  # noqa: E402,F401

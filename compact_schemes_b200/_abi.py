@@ -17,6 +17,7 @@ def declare(L):
     L.cs_numerics_destroy.argtypes = [vp]
     L.cs_deriv_setup.argtypes = [vp]
     L.cs_get_coeffs.argtypes = [vp, vp, vp]
+    L.cs_interface_coeffs.argtypes = [vp, vp]
     L.cs_get_ndf.argtypes = [vp, vp]
     L.cs_get_buffers.argtypes = [vp, i32, pp, pp, pp]
     L.cs_deriv.argtypes = [vp, i32, vp, vp, i32, i32, Dcomp, u32, u32, u32, i32, vp]
@@ -25,7 +26,23 @@ def declare(L):
     L.cs_halo_exchange_self.argtypes = [vp, u32, vp]
     L.cs_filter.argtypes = [vp, i32, vp, vp, f64, Dcomp, vp]
     L.cs_line_tables.argtypes = [i32, i32, i32, i32, f64, vp, vp, sz]
-    for name in ("cs_numerics_create", "cs_numerics_destroy", "cs_deriv_setup", "cs_get_coeffs",
+    from .solver import SolverConfig
+    L.cs_solver_create.argtypes = [pp, ctypes.POINTER(SolverConfig)]
+    L.cs_solver_destroy.argtypes = [vp]
+    L.cs_solver_rhs.argtypes = [vp, vp, vp, vp]
+    L.cs_solver_stage.argtypes = [vp, i32, vp, vp, vp, f64, vp]
+    L.cs_solver_step.argtypes = [vp, vp, f64, vp]
+    L.cs_solver_step_host.argtypes = [vp, vp, vp, f64, vp]
+    L.cs_solver_last_dt.argtypes = [vp, ctypes.POINTER(f64)]
+    L.cs_solver_dt_device.argtypes = [vp, pp]
+    L.cs_tgv_init.argtypes = [vp, i32, i32, i32, f64, f64, ctypes.c_uint64, vp]
+    L.cs_solver_profile_begin.argtypes = [vp]
+    L.cs_solver_profile_end.argtypes = [vp, vp, vp]
+    for name in ("cs_solver_create", "cs_solver_destroy", "cs_solver_rhs", "cs_solver_stage",
+                 "cs_solver_step", "cs_solver_step_host", "cs_solver_last_dt", "cs_solver_dt_device", "cs_tgv_init",
+                 "cs_solver_profile_begin", "cs_solver_profile_end",
+                 "cs_numerics_create", "cs_numerics_destroy", "cs_deriv_setup", "cs_get_coeffs",
+                 "cs_interface_coeffs",
                  "cs_get_ndf", "cs_get_buffers", "cs_deriv", "cs_deriv_f32", "cs_fill_buffers",
                  "cs_halo_exchange_self", "cs_filter", "cs_line_tables"):
         getattr(L, name).restype = i32

@@ -14,6 +14,7 @@ LIB = os.path.join(HERE, "libcompact_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+         "-Xcompiler", "-ffp-contract=off",
          "--expt-relaxed-constexpr", "-I" + os.path.join(os.path.dirname(HERE), "include")]
 
 

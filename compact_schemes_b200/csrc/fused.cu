@@ -1,0 +1,765 @@
+// fused.cu -- the fused RHS / RK-stage pipeline of compact_schemes_b200.
+//
+// One RK stage of the compressible Navier-Stokes RHS of the reference
+// (physics::calc_viscous_shear_stress + physics::calc_fluxes,
+// src/physics_pc.hpp:83-227, followed by the RK update that
+// physics_base::movef leaves empty, src/physics_base.hpp:147-150) runs as six
+// line-solve passes over the state, each staging a tile of full lines in
+// shared memory:
+//   grad pass a (a = x, y, z): q -> u, v, w, T on the fly -> 4 compact
+//       derivatives along a -> G[a] (4 fields).  The first pass of a step
+//       also reduces the two CFL maxima of calc_time_step.
+//   flux pass a: q, G -> tau, heat flux, flux F[m][a] (m = 0..4) on the fly
+//       -> 5 compact derivatives along a -> R (= for x, += for y) or, for the
+//       last axis, q_out = q^n - dt/(4-k) * J * (R + dF)  (RK update fused).
+// Metrics are those of a uniform Cartesian grid (constants, not read).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "context.h"
+#include "tile.cuh"
+
+namespace csb {
+
+struct Phys {
+    double M[3][3];  // metric rows xim, etm, zem (J^-1 grad xi_a)
+    double J;        // yaco
+    double mu;       // ssk (dynamic viscosity, constant)
+    double umf[3];   // moving-frame velocity
+    double rr1;      // sum of squared metric entries
+};
+
+struct RkParams {
+    double div;        // nkrk - k: stage coefficient dt / (nkrk - k)
+    double dt_fixed;   // > 0: use it; else CFL dt from dtacc
+    double cfl;
+    const unsigned long long *dtacc;  // two maxima as bit patterns of non-negative doubles
+    double *dt_out;
+};
+
+__device__ __forceinline__ double rk_dt(const RkParams &rk) {
+    if (rk.dt_fixed > 0.0) return rk.dt_fixed;
+    const double m1 = __longlong_as_double((long long)rk.dtacc[0]);
+    const double m2 = __longlong_as_double((long long)rk.dtacc[1]);
+    const double a = rk.cfl / m1, b = 0.5 / m2;
+    return a < b ? a : b;
+}
+
+// Primitive variables from the conserved state (CANARD units: T stored as
+// c^2 = gamma p / rho).
+struct Prim {
+    double rho, ri, u, v, w, p, T;
+};
+__device__ __forceinline__ Prim primitives(double q0, double q1, double q2, double q3, double q4) {
+    Prim s;
+    s.rho = q0;
+    s.ri = 1.0 / q0;
+    s.u = xmul(q1, s.ri);
+    s.v = xmul(q2, s.ri);
+    s.w = xmul(q3, s.ri);
+    s.p = xmul(kGamm1, q4 - xmul(0.5, xmul(q1, s.u) + xmul(q2, s.v) + xmul(q3, s.w)));
+    s.T = xmul(xmul(kGam, s.p), s.ri);
+    return s;
+}
+
+template <int LT>
+__device__ __forceinline__ double *field_line(double *sm, int field, int line) {
+    return sm + (field * kTileLines + line) * LineLayout<LT>::kSlot;
+}
+
+// Solve the derivative of nf fields of this warp's line held in shared memory
+// and overwrite them with the result.
+template <int LT, int NF>
+__device__ __forceinline__ void solve_fields(double *sm, int w, int lane, const DevTables<double> &tab,
+                                             int nstart, int nend, const Coeffs &cf) {
+#pragma unroll 1
+    for (int c = 0; c < NF; ++c) {
+        double *line = field_line<LT>(sm, c, w);
+        double d[1][LT];
+        deriv_rhs<LT, double, double>(line, tab.n, lane, nstart, nend, nullptr, cf, d[0]);
+        warp_solve<LT, 1, double>(tab, d, lane);
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < LT; ++t)
+            if (lane * LT + t < tab.n) line[LineLayout<LT>::pos_ct(lane, t)] = d[0][t];
+    }
+}
+
+// ----------------------------------------------------------------------------
+// gradient pass: G[AXIS][c] = d/dxi_AXIS of (u, v, w, T)
+// ----------------------------------------------------------------------------
+template <int LT, int AXIS, bool DTRED>
+__global__ void __launch_bounds__(kThreads, 2)
+k_grad(const double *__restrict__ q, double *__restrict__ g, DevTables<double> tab, int lxi, int let,
+       int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf, Phys ph,
+       unsigned long long *__restrict__ dtacc) {
+    using L = LineLayout<LT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sm = reinterpret_cast<double *>(smem_raw);
+    const int n = tab.n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t line0 = (int64_t)blockIdx.x * kTileLines;
+    double m1 = 0.0, m2 = 0.0;
+    tile_for_each<AXIS, 2>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        const Prim s = primitives(__ldg(q + gi), __ldg(q + lmx + gi), __ldg(q + 2 * lmx + gi),
+                                  __ldg(q + 3 * lmx + gi), __ldg(q + 4 * lmx + gi));
+        const int pj = L::pos(j);
+        field_line<LT>(sm, 0, l)[pj] = s.u;
+        field_line<LT>(sm, 1, l)[pj] = s.v;
+        field_line<LT>(sm, 2, l)[pj] = s.w;
+        field_line<LT>(sm, 3, l)[pj] = s.T;
+        if (DTRED) {
+            // calc_time_step_kernel (src/cuda/kernels/physics.hpp:335-427)
+            const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
+            double rr2 = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                rr2 += fabs(xmul(ph.M[a][0], uu) + xmul(ph.M[a][1], vv) + xmul(ph.M[a][2], ww));
+            const double ssi = fabs(ph.J);
+            const double v1 = xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi);
+            const double v2 = s.ri * ph.mu * ph.rr1 * ssi * ssi;
+            m1 = fmax(m1, v1);
+            m2 = fmax(m2, v2);
+        }
+    });
+    tile_sync<AXIS>();
+    const int64_t fidx = line0 + w;
+    if (fidx < F) solve_fields<LT, 4>(sm, w, lane, tab, nstart, nend, cf);
+    tile_sync<AXIS>();
+    tile_for_each<AXIS, 2>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        const int pj = L::pos(j);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) g[c * lmx + gi] = field_line<LT>(sm, c, l)[pj];
+    });
+    if (DTRED) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+            m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+        }
+        if (lane == 0) {
+            atomicMax(dtacc, (unsigned long long)__double_as_longlong(m1));
+            atomicMax(dtacc + 1, (unsigned long long)__double_as_longlong(m2));
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// flux pass
+// ----------------------------------------------------------------------------
+enum FluxMode { kWrite = 0, kAccum = 1, kAccumRk = 2, kWriteRk = 3 };
+
+// Flux components F[m][AXIS] at one point from the state and the gradients
+// (calc_fluxes_pre_compute_kernel<Visc>, src/cuda/kernels/physics.hpp:42-193,
+// with tau / heat flux of calc_viscous_shear_stress_final_kernel, :285-333).
+template <int AXIS, bool VISC>
+__device__ __forceinline__ void point_flux(const double *__restrict__ q, const double *__restrict__ g,
+                                           int64_t lmx, int64_t gi, const Phys &ph, double (&fl)[5]) {
+    const double q0 = __ldg(q + gi), q1 = __ldg(q + lmx + gi), q2 = __ldg(q + 2 * lmx + gi);
+    const double q3 = __ldg(q + 3 * lmx + gi), q4 = __ldg(q + 4 * lmx + gi);
+    double gr[12];
+    if (VISC) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gr[k] = __ldg(g + k * lmx + gi);
+    }
+    const Prim s = primitives(q0, q1, q2, q3, q4);
+    const double *Ma = ph.M[AXIS];
+    const double ss = xmul(Ma[0], s.u + ph.umf[0]) + xmul(Ma[1], s.v + ph.umf[1]) + xmul(Ma[2], s.w + ph.umf[2]);
+    fl[0] = xmul(q0, ss);
+    fl[1] = xmul(q1, ss) + xmul(Ma[0], s.p);
+    fl[2] = xmul(q2, ss) + xmul(Ma[1], s.p);
+    fl[3] = xmul(q3, ss) + xmul(Ma[2], s.p);
+    fl[4] = xmul(q4 + s.p, ss) -
+            xmul(s.p, xmul(ph.umf[0], Ma[0]) + xmul(ph.umf[1], Ma[1]) + xmul(ph.umf[2], Ma[2]));
+    if (VISC) {
+        // physical gradients without the J factor: dc/dx_k = sum_b M[b][k] G[b][c]
+        double dx[4][3];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                dx[c][k] = xmul(ph.M[0][k], gr[c]) + xmul(ph.M[1][k], gr[4 + c]) + xmul(ph.M[2][k], gr[8 + c]);
+        const double muj = xmul(ph.mu, ph.J);
+        const double kap = xmul(kGamm1Prndtli, muj);
+        const double div = xmul(2.0 / 3.0, dx[0][0] + dx[1][1] + dx[2][2]);
+        const double txx = xmul(muj, xmul(2.0, dx[0][0]) - div);
+        const double tyy = xmul(muj, xmul(2.0, dx[1][1]) - div);
+        const double tzz = xmul(muj, xmul(2.0, dx[2][2]) - div);
+        const double txy = xmul(muj, dx[1][0] + dx[0][1]);
+        const double tyz = xmul(muj, dx[2][1] + dx[1][2]);
+        const double tzx = xmul(muj, dx[0][2] + dx[2][0]);
+        const double hx = xmul(kap, dx[3][0]) + xmul(s.u, txx) + xmul(s.v, txy) + xmul(s.w, tzx);
+        const double hy = xmul(kap, dx[3][1]) + xmul(s.u, txy) + xmul(s.v, tyy) + xmul(s.w, tyz);
+        const double hz = xmul(kap, dx[3][2]) + xmul(s.u, tzx) + xmul(s.v, tyz) + xmul(s.w, tzz);
+        fl[1] -= xmul(Ma[0], txx) + xmul(Ma[1], txy) + xmul(Ma[2], tzx);
+        fl[2] -= xmul(Ma[0], txy) + xmul(Ma[1], tyy) + xmul(Ma[2], tyz);
+        fl[3] -= xmul(Ma[0], tzx) + xmul(Ma[1], tyz) + xmul(Ma[2], tzz);
+        fl[4] -= xmul(Ma[0], hx) + xmul(Ma[1], hy) + xmul(Ma[2], hz);
+    }
+}
+
+template <int LT, int AXIS, int MODE, bool VISC>
+__global__ void __launch_bounds__(kThreads, 2)
+k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__restrict__ rhs,
+       const double *__restrict__ qn, double *__restrict__ qout, double *__restrict__ drva,
+       DevTables<double> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend,
+       Coeffs cf, Phys ph, RkParams rk) {
+    using L = LineLayout<LT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sm = reinterpret_cast<double *>(smem_raw);
+    const int n = tab.n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t line0 = (int64_t)blockIdx.x * kTileLines;
+    tile_for_each<AXIS, 1>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        double fl[5];
+        point_flux<AXIS, VISC>(q, g, lmx, gi, ph, fl);
+        const int pj = L::pos(j);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) field_line<LT>(sm, m, l)[pj] = fl[m];
+    });
+    tile_sync<AXIS>();
+    const int64_t fidx = line0 + w;
+    if (fidx < F) {
+        solve_fields<LT, 5>(sm, w, lane, tab, nstart, nend, cf);
+        if (drva) {
+            // line-end derivatives for the characteristic boundary closure
+            // (drva of deriv_kernel_2d, src/cuda/kernels/numerics_pc.hpp:237-248)
+            __syncwarp();
+            if (lane < 10) {
+                const int m = lane % 5, face = lane / 5;
+                drva[(int64_t)(face * 5 + m) * F + fidx] = field_line<LT>(sm, m, w)[L::pos(face ? n - 1 : 0)];
+            }
+        }
+    }
+    tile_sync<AXIS>();
+    double dtk = 0.0;
+    if (MODE >= kAccumRk) {
+        const double dt = rk_dt(rk);
+        dtk = xmul(dt / rk.div, ph.J);
+        if (rk.dt_out && blockIdx.x == 0 && threadIdx.x == 0) *rk.dt_out = dt;
+    }
+    tile_for_each<AXIS, 1>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        const int pj = L::pos(j);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            const double dfv = field_line<LT>(sm, m, l)[pj];
+            if (MODE == kWrite) rhs[m * lmx + gi] = dfv;
+            else if (MODE == kAccum) rhs[m * lmx + gi] += dfv;
+            else {
+                const double r = MODE == kAccumRk ? rhs[m * lmx + gi] + dfv : dfv;
+                qout[m * lmx + gi] = qn[m * lmx + gi] - xmul(dtk, r);
+            }
+        }
+    });
+}
+
+// ----------------------------------------------------------------------------
+// GCBC, non-reflective, x faces (gcbc_setup_kernel + gcbc_update_non_reflective_kernel,
+// src/cuda/kernels/gcbc.hpp:251-454, reference defects fixed: see oracle/oracle.cpp)
+// ----------------------------------------------------------------------------
+__global__ void k_gcbc_x(double *__restrict__ rhs, const double *__restrict__ drva,
+                         const double *__restrict__ q, int lxi, int64_t lmx, int64_t F, int face_mask,
+                         Phys ph, double sb0, double sb1, double sb2, double sb3) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * F) return;
+    const int ip = (int)(t / F);
+    const int64_t fi = t % F;
+    if (!((face_mask >> ip) & 1)) return;
+    const int64_t idx = fi * lxi + (ip ? lxi - 1 : 0);
+    // face normal: grad(xi) / |grad(xi)| (exactly (+-1, 0, 0) on a Cartesian grid)
+    double c[3];
+    if (ph.M[0][1] == 0.0 && ph.M[0][2] == 0.0) {
+        c[0] = ph.M[0][0] > 0.0 ? 1.0 : -1.0; c[1] = 0.0; c[2] = 0.0;
+    } else {
+        const double nrm = sqrt(xmul(ph.M[0][0], ph.M[0][0]) + xmul(ph.M[0][1], ph.M[0][1]) +
+                                xmul(ph.M[0][2], ph.M[0][2]));
+        c[0] = ph.M[0][0] / nrm; c[1] = ph.M[0][1] / nrm; c[2] = ph.M[0][2] / nrm;
+    }
+    const double rho = q[idx], rhoi = 1.0 / rho;
+    const double ve[3] = {xmul(q[lmx + idx], rhoi), xmul(q[2 * lmx + idx], rhoi), xmul(q[3 * lmx + idx], rhoi)};
+    const double hv2 = xmul(0.5, xmul(ve[0], ve[0]) + xmul(ve[1], ve[1]) + xmul(ve[2], ve[2]));
+    const double pp = xmul(kGamm1, q[4 * lmx + idx] - xmul(rho, hv2));
+    const double ao = sqrt(xmul(xmul(kGam, rhoi), pp)), aoi = 1.0 / ao;
+    const double vn = xmul(c[0], ve[0]) + xmul(c[1], ve[1]) + xmul(c[2], ve[2]);
+    const double vs = xmul(c[0], ph.umf[0]) + xmul(c[1], ph.umf[1]) + xmul(c[2], ph.umf[2]);
+    double dr[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) dr[v] = xmul(ph.J, drva[(int64_t)(ip * 5 + v) * F + fi]);
+    // characteristic amplitudes of the two acoustic waves (rows 3, 4 of xtq2r)
+    const double ho = xmul(xmul(kGamm1, aoi), aoi), bo = 1.0 - xmul(ho, hv2), co = xmul(aoi, vn);
+    const double dm[3] = {xmul(aoi, c[0]), xmul(aoi, c[1]), xmul(aoi, c[2])};
+    const double rv[3] = {xmul(ho, ve[0]), xmul(ho, ve[1]), xmul(ho, ve[2])};
+    const double cha3 = xmul(1.0 - bo - co, dr[0]) + xmul(dm[0] - rv[0], dr[1]) + xmul(dm[1] - rv[1], dr[2]) +
+                        xmul(dm[2] - rv[2], dr[3]) + xmul(ho, dr[4]);
+    const double cha4 = xmul(1.0 - bo + co, dr[0]) + xmul(-dm[0] - rv[0], dr[1]) + xmul(-dm[1] - rv[1], dr[2]) +
+                        xmul(-dm[2] - rv[2], dr[3]) + xmul(ho, dr[4]);
+    const double ra0 = 1.0 - 2.0 * ip;
+    const double d3 = ra0 * (vn + vs + ao) > 0 ? -cha3 : 0.0;
+    const double d4 = ra0 * (vn + vs - ao) > 0 ? -cha4 : 0.0;
+    // back to conservative variables: columns 3, 4 of xtr2q
+    const double bo2 = hv2 + xmul(xmul(kHamm1, ao), ao), co2 = xmul(ao, vn);
+    const double em[3] = {xmul(ao, c[0]), xmul(ao, c[1]), xmul(ao, c[2])};
+    double dq[5];
+    dq[0] = xmul(0.5, d3) + xmul(0.5, d4);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double s3 = xmul(0.5, ve[k] + em[k]);
+        dq[1 + k] = xmul(s3, d3) + xmul(s3 - em[k], d4);
+    }
+    {
+        const double s3 = xmul(0.5, bo2 + co2);
+        dq[4] = xmul(s3, d3) + xmul(s3 - co2, d4);
+    }
+    const double sb[4] = {sb0, sb1, sb2, sb3};
+    const int iq = 1 - 2 * ip;
+#pragma unroll
+    for (int ii = 0; ii < kMbci; ++ii) {
+        if (sb[ii] == 0.0) continue;
+        const int64_t o = idx + (int64_t)ii * iq;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) rhs[v * lmx + o] += xmul(sb[ii], dq[v]);
+    }
+}
+
+// Taylor-Green initial state (see oracle or_tgv_init for the definition).
+__device__ __forceinline__ double noise01(uint64_t seed, uint64_t index) {
+    uint64_t z = seed * 0x9E3779B97F4A7C15ull + index + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+__global__ void k_tgv(double *__restrict__ q, int lxi, int let, int64_t lmx, double mach, double amp,
+                      uint64_t seed, double hx, double hy, double hz) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= lmx) return;
+    const int64_t i = idx % lxi, j = (idx / lxi) % let, k = idx / ((int64_t)lxi * let);
+    const double x = i * hx, y = j * hy, z = k * hz;
+    const double u = mach * sin(x) * cos(y) * cos(z);
+    const double v = -mach * cos(x) * sin(y) * cos(z);
+    const double w = 0.0;
+    const double p = 1.0 / kGam + mach * mach / 16.0 * (cos(2 * x) + cos(2 * y)) * (cos(2 * z) + 2.0);
+    const double rho = 1.0 + amp * noise01(seed, (uint64_t)idx);
+    q[idx] = rho;
+    q[lmx + idx] = rho * u;
+    q[2 * lmx + idx] = rho * v;
+    q[3 * lmx + idx] = rho * w;
+    q[4 * lmx + idx] = p * kHamm1 + 0.5 * rho * (u * u + v * v + w * w);
+}
+
+// ----------------------------------------------------------------------------
+// host side
+// ----------------------------------------------------------------------------
+template <typename KernelT>
+static int set_smem(KernelT kern, size_t bytes) {
+    if (bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+    }
+    return CS_OK;
+}
+
+}  // namespace csb
+
+using namespace csb;
+
+struct cs_solver {
+    cs_solver_config cfg{};
+    cs_dcomp d{};
+    int ndf[2][3]{};
+    Coeffs cf{};
+    Phys ph{};
+    TableCache tables;
+    const DeviceTables *tab[3] = {nullptr, nullptr, nullptr};
+    int active[3] = {0, 0, 0};
+    double *q1 = nullptr, *grad = nullptr, *rhs = nullptr, *drva = nullptr;
+    double *qhost_dev = nullptr;  // device state for cs_solver_step_host
+    unsigned long long *dtacc = nullptr;
+    double *dt_dev = nullptr;
+    int64_t F[3] = {0, 0, 0};
+    // optional per-pass event timing (eager path only)
+    bool profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof;
+    std::vector<cudaEvent_t> event_pool;
+    // captured step graph
+    cudaGraphExec_t graph = nullptr;
+    const double *graph_q = nullptr;
+    double graph_dt = 0.0;
+    cudaStream_t graph_stream = nullptr;
+};
+
+namespace csb {
+
+// Pass kinds reported by cs_solver_profile_end.
+enum PassKind { kPassGradX = 0, kPassGradY, kPassGradZ, kPassFluxX, kPassFluxY, kPassFluxZ, kPassGcbc,
+                kPassKinds };
+
+static cudaEvent_t take_event(cs_solver *s) {
+    if (!s->event_pool.empty()) {
+        cudaEvent_t e = s->event_pool.back();
+        s->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// RAII bracket: records a start/stop event pair around one pass when profiling.
+struct PassTimer {
+    cs_solver *s;
+    cudaStream_t st;
+    int kind;
+    cudaEvent_t a = nullptr, b = nullptr;
+    PassTimer(cs_solver *s_, cudaStream_t st_, int kind_) : s(s_), st(st_), kind(kind_) {
+        if (s->profiling) {
+            a = take_event(s);
+            b = take_event(s);
+            cudaEventRecord(a, st);
+        }
+    }
+    ~PassTimer() {
+        if (s->profiling) {
+            cudaEventRecord(b, st);
+            s->prof.push_back({kind, {a, b}});
+        }
+    }
+};
+
+static int64_t fsize(const cs_dcomp &d, int a) {
+    return a == 0 ? (int64_t)d.let * d.lze : (a == 1 ? (int64_t)d.lxi * d.lze : (int64_t)d.lxi * d.let);
+}
+static int llen(const cs_dcomp &d, int a) { return a == 0 ? d.lxi : (a == 1 ? d.let : d.lze); }
+
+template <int LT, int AXIS>
+static int launch_grad_lt(cs_solver *s, const double *q, bool dtred, cudaStream_t st) {
+    const size_t smem = (size_t)4 * kTileLines * LineLayout<LT>::kSlot * sizeof(double);
+    auto kern = dtred ? k_grad<LT, AXIS, true> : k_grad<LT, AXIS, false>;
+    if (int rc = set_smem(kern, smem)) return rc;
+    const int64_t F = s->F[AXIS];
+    const unsigned blocks = (unsigned)((F + kTileLines - 1) / kTileLines);
+    kern<<<blocks, kThreads, smem, st>>>(q, s->grad + (int64_t)AXIS * 4 * s->d.lmx, s->tab[AXIS]->t64,
+                                         s->d.lxi, s->d.let, s->d.lmx, F, s->ndf[0][AXIS],
+                                         s->ndf[1][AXIS], s->cf, s->ph, s->dtacc);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+template <int AXIS>
+static int launch_grad(cs_solver *s, const double *q, bool dtred, cudaStream_t st) {
+    switch (s->tab[AXIS]->lt) {
+        case 2: return launch_grad_lt<2, AXIS>(s, q, dtred, st);
+        case 4: return launch_grad_lt<4, AXIS>(s, q, dtred, st);
+        case 8: return launch_grad_lt<8, AXIS>(s, q, dtred, st);
+        case 16: return launch_grad_lt<16, AXIS>(s, q, dtred, st);
+        case 32: return launch_grad_lt<32, AXIS>(s, q, dtred, st);
+    }
+    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
+}
+
+static int grad_pass(cs_solver *s, int a, const double *q, bool dtred, cudaStream_t st) {
+    PassTimer pt(s, st, kPassGradX + a);
+    if (a == 0) return launch_grad<0>(s, q, dtred, st);
+    if (a == 1) return launch_grad<1>(s, q, dtred, st);
+    return launch_grad<2>(s, q, dtred, st);
+}
+
+template <int LT, int AXIS, int MODE>
+static int launch_flux_lt(cs_solver *s, const double *q, const double *qn, double *qout, double *drva,
+                          const RkParams &rk, cudaStream_t st) {
+    const size_t smem = (size_t)5 * kTileLines * LineLayout<LT>::kSlot * sizeof(double);
+    auto kern = s->cfg.viscous ? k_flux<LT, AXIS, MODE, true> : k_flux<LT, AXIS, MODE, false>;
+    if (int rc = set_smem(kern, smem)) return rc;
+    const int64_t F = s->F[AXIS];
+    const unsigned blocks = (unsigned)((F + kTileLines - 1) / kTileLines);
+    kern<<<blocks, kThreads, smem, st>>>(q, s->grad, s->rhs, qn, qout, drva, s->tab[AXIS]->t64, s->d.lxi,
+                                         s->d.let, s->d.lmx, F, s->ndf[0][AXIS], s->ndf[1][AXIS], s->cf,
+                                         s->ph, rk);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+template <int AXIS, int MODE>
+static int launch_flux_m(cs_solver *s, const double *q, const double *qn, double *qout, double *drva,
+                         const RkParams &rk, cudaStream_t st) {
+    switch (s->tab[AXIS]->lt) {
+        case 2: return launch_flux_lt<2, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
+        case 4: return launch_flux_lt<4, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
+        case 8: return launch_flux_lt<8, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
+        case 16: return launch_flux_lt<16, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
+        case 32: return launch_flux_lt<32, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
+    }
+    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
+}
+
+template <int AXIS>
+static int launch_flux(cs_solver *s, int mode, const double *q, const double *qn, double *qout,
+                       double *drva, const RkParams &rk, cudaStream_t st) {
+    switch (mode) {
+        case kWrite: return launch_flux_m<AXIS, kWrite>(s, q, qn, qout, drva, rk, st);
+        case kAccum: return launch_flux_m<AXIS, kAccum>(s, q, qn, qout, drva, rk, st);
+        case kAccumRk: return launch_flux_m<AXIS, kAccumRk>(s, q, qn, qout, drva, rk, st);
+        default: return launch_flux_m<AXIS, kWriteRk>(s, q, qn, qout, drva, rk, st);
+    }
+}
+
+static int flux_pass(cs_solver *s, int a, int mode, const double *q, const double *qn, double *qout,
+                     double *drva, const RkParams &rk, cudaStream_t st) {
+    PassTimer pt(s, st, kPassFluxX + a);
+    if (a == 0) return launch_flux<0>(s, mode, q, qn, qout, drva, rk, st);
+    if (a == 1) return launch_flux<1>(s, mode, q, qn, qout, drva, rk, st);
+    return launch_flux<2>(s, mode, q, qn, qout, drva, rk, st);
+}
+
+static bool gcbc_on(const cs_solver *s) {
+    return s->cfg.gcbc && s->active[0] &&
+           (s->cfg.nbc[0][0] == CS_BC_NON_REFLECTIVE || s->cfg.nbc[1][0] == CS_BC_NON_REFLECTIVE);
+}
+
+// RHS of one state (rk == nullptr) or one full RK stage.
+static int run_stage(cs_solver *s, const double *qin, const double *qn, double *qout, double *rhs_out,
+                     const RkParams *rk, bool dtred, cudaStream_t st) {
+    int axes[3], na = 0;
+    for (int a = 0; a < 3; ++a)
+        if (s->active[a]) axes[na++] = a;
+    if (s->cfg.viscous)
+        for (int i = 0; i < na; ++i)
+            if (int rc = grad_pass(s, axes[i], qin, dtred && i == 0, st)) return rc;
+    if (dtred && !s->cfg.viscous) {
+        // inviscid: the CFL maxima come from a gradient-free reduction; reuse
+        // the x gradient pass into scratch (its output is unused)
+        if (int rc = grad_pass(s, axes[0], qin, true, st)) return rc;
+    }
+    double *saved_rhs = s->rhs;
+    if (rhs_out) s->rhs = rhs_out;
+    RkParams none{};
+    for (int i = 0; i < na; ++i) {
+        const int a = axes[i];
+        int mode;
+        if (!rk) mode = i == 0 ? kWrite : kAccum;
+        else if (na == 1) mode = kWriteRk;
+        else mode = i == 0 ? kWrite : (i == na - 1 ? kAccumRk : kAccum);
+        double *drva = (a == 0 && gcbc_on(s)) ? s->drva : nullptr;
+        int rc = flux_pass(s, a, mode, qin, qn, qout, drva, rk ? *rk : none, st);
+        if (rc) { s->rhs = saved_rhs; return rc; }
+        if (drva && (mode == kWrite || mode == kAccum) && !(rk && na == 1)) {
+            PassTimer pt(s, st, kPassGcbc);
+            const int64_t F = s->F[0];
+            int mask = (s->cfg.nbc[0][0] == CS_BC_NON_REFLECTIVE ? 1 : 0) |
+                       (s->cfg.nbc[1][0] == CS_BC_NON_REFLECTIVE ? 2 : 0);
+            k_gcbc_x<<<(unsigned)((2 * F + 127) / 128), 128, 0, st>>>(s->rhs, s->drva, qin, s->d.lxi,
+                                                                    s->d.lmx, F, mask, s->ph,
+                                                                    1.0 / s->ph.J, 0.0, 0.0, 0.0);
+            if (cudaGetLastError() != cudaSuccess) { s->rhs = saved_rhs; return set_error(CS_ERR_CUDA, "gcbc launch"); }
+        }
+    }
+    s->rhs = saved_rhs;
+    return CS_OK;
+}
+
+static int run_step(cs_solver *s, double *q, double dt, cudaStream_t st) {
+    const bool cfl = !(dt > 0.0);
+    if (cfl) CSB_CUDA(cudaMemsetAsync(s->dtacc, 0, 2 * sizeof(unsigned long long), st));
+    for (int k = 0; k < 4; ++k) {
+        RkParams rk{};
+        rk.div = 4 - k;
+        rk.dt_fixed = cfl ? 0.0 : dt;
+        rk.cfl = s->cfg.cfl;
+        rk.dtacc = s->dtacc;
+        rk.dt_out = k == 0 ? s->dt_dev : nullptr;
+        const double *qin = k == 0 ? q : s->q1;
+        double *qout = k == 3 ? q : s->q1;
+        if (int rc = run_stage(s, qin, q, qout, nullptr, &rk, cfl && k == 0, st)) return rc;
+    }
+    return CS_OK;
+}
+
+}  // namespace csb
+
+extern "C" {
+
+int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
+    if (!out || !cfg) return set_error(CS_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (cfg->lxi < 1 || cfg->let < 1 || cfg->lze < 1) return set_error(CS_ERR_INVALID, "dims");
+    if (!(cfg->dx > 0 && cfg->dy > 0 && cfg->dz > 0)) return set_error(CS_ERR_INVALID, "grid spacing");
+    auto *s = new cs_solver();
+    s->cfg = *cfg;
+    s->d = cs_dcomp{cfg->lxi * cfg->let * cfg->lze, cfg->lxi, cfg->let, cfg->lze};
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 3; ++a) {
+            const int b = cfg->nbc[f][a];
+            if (b == CS_BC_NON_REFLECTIVE || b == CS_BC_WALL_INVISCID || b == CS_BC_WALL_VISCOUS ||
+                b == CS_BC_INTER_CURV) s->ndf[f][a] = 0;
+            else if (b == CS_BC_INTER_STRAIGHT || b == CS_BC_INTER_SUBDOMAINS || b == CS_BC_PERIODIC)
+                s->ndf[f][a] = 1;
+            else { delete s; return set_error(CS_ERR_INVALID, "boundary code %d", b); }
+        }
+    for (int a = 0; a < 3; ++a) {
+        const int n = llen(s->d, a);
+        s->F[a] = fsize(s->d, a);
+        if (n == 1) continue;  // degenerate axis: no derivative along it
+        if (s->ndf[0][a] != s->ndf[1][a]) {
+            delete s;
+            return set_error(CS_ERR_UNSUPPORTED, "axis %d: a single rank needs both faces periodic or both physical", a);
+        }
+        if (n < 5 || (s->ndf[0][a] && n < kLmd)) { delete s; return set_error(CS_ERR_UNSUPPORTED, "axis %d too short", a); }
+        s->tab[a] = s->tables.get(n, kDeriv, s->ndf[0][a], s->ndf[1][a], 0.0);
+        if (!s->tab[a]) { delete s; return CS_ERR_UNSUPPORTED; }
+        s->active[a] = 1;
+    }
+    compute_interface_coeffs(s->cf);
+    const double hx = cfg->dx, hy = cfg->dy, hz = cfg->dz;
+    std::memset(&s->ph, 0, sizeof s->ph);
+    s->ph.M[0][0] = hy * hz;
+    s->ph.M[1][1] = hx * hz;
+    s->ph.M[2][2] = hx * hy;
+    s->ph.J = 1.0 / (hx * hy * hz);
+    s->ph.mu = cfg->mu;
+    for (int c = 0; c < 3; ++c) s->ph.umf[c] = cfg->umf[c];
+    s->ph.rr1 = s->ph.M[0][0] * s->ph.M[0][0] + s->ph.M[1][1] * s->ph.M[1][1] + s->ph.M[2][2] * s->ph.M[2][2];
+    const int64_t lmx = s->d.lmx;
+    bool ok = cudaMalloc(&s->q1, 5 * lmx * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&s->grad, 12 * lmx * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&s->rhs, 5 * lmx * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&s->drva, 10 * s->F[0] * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&s->dtacc, 2 * sizeof(unsigned long long)) == cudaSuccess &&
+              cudaMalloc(&s->dt_dev, sizeof(double)) == cudaSuccess;
+    if (!ok) {
+        cs_solver_destroy(s);
+        return set_error(CS_ERR_ALLOC, "solver scratch allocation failed");
+    }
+    cudaMemset(s->grad, 0, 12 * lmx * sizeof(double));
+    cudaMemset(s->dtacc, 0, 2 * sizeof(unsigned long long));
+    cudaMemset(s->dt_dev, 0, sizeof(double));
+    *out = s;
+    return CS_OK;
+}
+
+int cs_solver_profile_begin(cs_solver *s) {
+    if (!s) return set_error(CS_ERR_INVALID, "null argument");
+    for (auto &p : s->prof) {
+        s->event_pool.push_back(p.second.first);
+        s->event_pool.push_back(p.second.second);
+    }
+    s->prof.clear();
+    s->profiling = true;
+    return CS_OK;
+}
+
+int cs_solver_profile_end(cs_solver *s, double ms[CS_PASS_KINDS], int launches[CS_PASS_KINDS]) {
+    if (!s || !ms || !launches) return set_error(CS_ERR_INVALID, "null argument");
+    s->profiling = false;
+    for (int k = 0; k < kPassKinds; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    for (auto &p : s->prof) {
+        CSB_CUDA(cudaEventSynchronize(p.second.second));
+        float t = 0.f;
+        CSB_CUDA(cudaEventElapsedTime(&t, p.second.first, p.second.second));
+        ms[p.first] += t;
+        launches[p.first] += 1;
+    }
+    return CS_OK;
+}
+
+int cs_solver_destroy(cs_solver *s) {
+    if (!s) return CS_OK;
+    for (auto &p : s->prof) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    for (auto e : s->event_pool) cudaEventDestroy(e);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    for (void *p : {(void *)s->q1, (void *)s->grad, (void *)s->rhs, (void *)s->drva, (void *)s->dtacc,
+                    (void *)s->dt_dev, (void *)s->qhost_dev})
+        if (p) cudaFree(p);
+    delete s;
+    return CS_OK;
+}
+
+int cs_solver_rhs(cs_solver *s, const double *q, double *rhs, void *stream) {
+    if (!s || !q || !rhs) return set_error(CS_ERR_INVALID, "null argument");
+    return run_stage(s, q, q, nullptr, rhs, nullptr, false, (cudaStream_t)stream);
+}
+
+int cs_solver_stage(cs_solver *s, int k, const double *qn, const double *qin, double *qout, double dt,
+                    void *stream) {
+    if (!s || !qn || !qin || !qout || k < 0 || k > 3 || !(dt > 0.0))
+        return set_error(CS_ERR_INVALID, "bad argument");
+    RkParams rk{};
+    rk.div = 4 - k;
+    rk.dt_fixed = dt;
+    rk.cfl = s->cfg.cfl;
+    rk.dtacc = s->dtacc;
+    return run_stage(s, qin, qn, qout, nullptr, &rk, false, (cudaStream_t)stream);
+}
+
+int cs_solver_step(cs_solver *s, double *q, double dt, void *stream) {
+    if (!s || !q) return set_error(CS_ERR_INVALID, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (s->cfg.use_graph && !s->profiling) {
+        if (!s->graph || s->graph_q != q || s->graph_dt != dt || s->graph_stream != st) {
+            if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
+            cudaStream_t cap;
+            CSB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            cudaGraph_t g;
+            CSB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+            int rc = run_step(s, q, dt, cap);
+            cudaError_t e = cudaStreamEndCapture(cap, &g);
+            cudaStreamDestroy(cap);
+            if (rc) return rc;
+            if (e != cudaSuccess) return check_cuda(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&s->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { s->graph = nullptr; return check_cuda(e, "cudaGraphInstantiate"); }
+            s->graph_q = q;
+            s->graph_dt = dt;
+            s->graph_stream = st;
+        }
+        CSB_CUDA(cudaGraphLaunch(s->graph, st));
+        return CS_OK;
+    }
+    return run_step(s, q, dt, st);
+}
+
+int cs_solver_step_host(cs_solver *s, const double *q_in_host, double *q_out_host, double dt,
+                        void *stream) {
+    if (!s || !q_in_host || !q_out_host) return set_error(CS_ERR_INVALID, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = (size_t)5 * s->d.lmx * sizeof(double);
+    if (!s->qhost_dev && cudaMalloc(&s->qhost_dev, bytes) != cudaSuccess) {
+        s->qhost_dev = nullptr;
+        return set_error(CS_ERR_ALLOC, "state allocation failed");
+    }
+    CSB_CUDA(cudaMemcpyAsync(s->qhost_dev, q_in_host, bytes, cudaMemcpyHostToDevice, st));
+    if (int rc = cs_solver_step(s, s->qhost_dev, dt, stream)) return rc;
+    CSB_CUDA(cudaMemcpyAsync(q_out_host, s->qhost_dev, bytes, cudaMemcpyDeviceToHost, st));
+    CSB_CUDA(cudaStreamSynchronize(st));
+    return CS_OK;
+}
+
+int cs_solver_last_dt(cs_solver *s, double *dt) {
+    if (!s || !dt) return set_error(CS_ERR_INVALID, "null argument");
+    CSB_CUDA(cudaMemcpy(dt, s->dt_dev, sizeof(double), cudaMemcpyDeviceToHost));
+    return CS_OK;
+}
+
+int cs_solver_dt_device(cs_solver *s, double **dt_dev) {
+    if (!s || !dt_dev) return set_error(CS_ERR_INVALID, "null argument");
+    *dt_dev = s->dt_dev;
+    return CS_OK;
+}
+
+int cs_tgv_init(double *q, int lxi, int let, int lze, double mach, double noise_amp, uint64_t seed,
+                void *stream) {
+    if (!q || lxi < 1 || let < 1 || lze < 1) return set_error(CS_ERR_INVALID, "bad argument");
+    const int64_t lmx = (int64_t)lxi * let * lze;
+    const double tp = 6.283185307179586476925286766559;
+    k_tgv<<<(unsigned)((lmx + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        q, lxi, let, lmx, mach, noise_amp, seed, tp / lxi, tp / let, tp / lze);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+}  // extern "C"

@@ -20,6 +20,13 @@
 
 namespace csb {
 
+// Round-to-nearest products that the compiler may not contract into FMAs:
+// the pointwise arithmetic (fluxes, primitives, stencil right-hand sides) is
+// written with them in the operation order of a plain C++ evaluation, so its
+// results are bit-identical to the FP64 oracle built without contraction.
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+
 template <typename CT>
 struct DevTables {
     const CT *fwd1, *fwd2, *bwd1, *bwd2, *rca, *rcc, *k1, *k2, *invb, *cycz;
@@ -165,7 +172,7 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
     }
 #pragma unroll
     for (int t = 0; t < LT; ++t)
-        d[t] = (j0 + t < n) ? CT(kAa) * (w[t + 3] - w[t + 1]) + CT(kBb) * (w[t + 4] - w[t]) : CT(0);
+        d[t] = (j0 + t < n) ? xmul(CT(kAa), w[t + 3] - w[t + 1]) + xmul(CT(kBb), w[t + 4] - w[t]) : CT(0);
 
     const bool own_lo = lane == 0;
     const int own_hi1 = (n - 1) / LT, own_hi2 = (n - 2) / LT;
@@ -174,8 +181,8 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
         if (own_lo) {
             const CT f0 = CT(f[L::pos(0)]), f1 = CT(f[L::pos(1)]), f2 = CT(f[L::pos(2)]);
             if (nstart == 0) {
-                d[0] = CT(kAb00) * f0 + CT(kAb01) * f1 + CT(kAb02) * f2;
-                d[1] = CT(kAb10) * (f2 - f0);
+                d[0] = xmul(CT(kAb00), f0) + xmul(CT(kAb01), f1) + xmul(CT(kAb02), f2);
+                d[1] = xmul(CT(kAb10), f2 - f0);
             } else {
                 CT r0, r1;
                 if (recv4_or_null) {
@@ -185,15 +192,15 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
                     r0 = CT(0);
                     r1 = CT(0);
 #pragma unroll
-                    for (int k = 0; k < kLmd; ++k) r0 += CT(cf.pbco[k]) * CT(f[L::pos(n - 1 - k)]);
+                    for (int k = 0; k < kLmd; ++k) r0 += xmul(CT(cf.pbco[k]), CT(f[L::pos(n - 1 - k)]));
 #pragma unroll
-                    for (int k = 0; k < kLmd; ++k) r1 += CT(cf.pbco[kLmd + k]) * CT(f[L::pos(n - 1 - k)]);
+                    for (int k = 0; k < kLmd; ++k) r1 += xmul(CT(cf.pbco[kLmd + k]), CT(f[L::pos(n - 1 - k)]));
                 }
                 CT s0 = CT(0), s1 = CT(0);
 #pragma unroll
-                for (int k = 0; k < kLmd; ++k) s0 += CT(cf.pbci[k]) * CT(f[L::pos(k)]);
+                for (int k = 0; k < kLmd; ++k) s0 += xmul(CT(cf.pbci[k]), CT(f[L::pos(k)]));
 #pragma unroll
-                for (int k = 0; k < kLmd; ++k) s1 += CT(cf.pbci[kLmd + k]) * CT(f[L::pos(k)]);
+                for (int k = 0; k < kLmd; ++k) s1 += xmul(CT(cf.pbci[kLmd + k]), CT(f[L::pos(k)]));
                 d[0] = s0 + r0;
                 d[1] = s1 + r1;
             }
@@ -202,8 +209,8 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
             const CT g0 = CT(f[L::pos(n - 1)]), g1 = CT(f[L::pos(n - 2)]), g2 = CT(f[L::pos(n - 3)]);
             CT e1, e2;  // rows n-1 and n-2
             if (nend == 0) {
-                e1 = -(CT(kAb00) * g0 + CT(kAb01) * g1 + CT(kAb02) * g2);
-                e2 = -CT(kAb10) * (g2 - g0);
+                e1 = -(xmul(CT(kAb00), g0) + xmul(CT(kAb01), g1) + xmul(CT(kAb02), g2));
+                e2 = xmul(-CT(kAb10), g2 - g0);
             } else {
                 CT r2, r3;
                 if (recv4_or_null) {
@@ -213,16 +220,16 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
                     r2 = CT(0);
                     r3 = CT(0);
 #pragma unroll
-                    for (int k = 0; k < kLmd; ++k) r2 += CT(cf.pbco[k]) * CT(f[L::pos(k)]);
+                    for (int k = 0; k < kLmd; ++k) r2 += xmul(CT(cf.pbco[k]), CT(f[L::pos(k)]));
 #pragma unroll
-                    for (int k = 0; k < kLmd; ++k) r3 += CT(cf.pbco[kLmd + k]) * CT(f[L::pos(k)]);
+                    for (int k = 0; k < kLmd; ++k) r3 += xmul(CT(cf.pbco[kLmd + k]), CT(f[L::pos(k)]));
                 }
                 CT s0 = CT(0), s1 = CT(0);
 #pragma unroll
-                for (int k = 0; k < kLmd; ++k) s0 += CT(cf.pbci[k]) * CT(f[L::pos(n - 1 - k)]);
+                for (int k = 0; k < kLmd; ++k) s0 += xmul(CT(cf.pbci[k]), CT(f[L::pos(n - 1 - k)]));
                 s0 += r2;
 #pragma unroll
-                for (int k = 0; k < kLmd; ++k) s1 += CT(cf.pbci[kLmd + k]) * CT(f[L::pos(n - 1 - k)]);
+                for (int k = 0; k < kLmd; ++k) s1 += xmul(CT(cf.pbci[kLmd + k]), CT(f[L::pos(n - 1 - k)]));
                 s1 += r3;
                 e1 = -s0;
                 e2 = -s1;
@@ -241,11 +248,13 @@ template <int LT, typename CT, typename FT>
 __device__ __forceinline__ void filter_rhs(const FT *f, int n, int lane, bool cyclic, CT af,
                                            CT (&d)[LT]) {
     using L = LineLayout<LT>;
-    const CT a60 = (CT(11) + CT(10) * af) / CT(16), a61 = (CT(15) + CT(34) * af) / CT(32);
-    const CT a62 = (CT(-3) + CT(6) * af) / CT(16), a63 = (CT(1) - CT(2) * af) / CT(32);
-    const CT a40 = (CT(5) + CT(6) * af) / CT(8), a41 = (CT(1) + CT(2) * af) / CT(2);
-    const CT a42 = (CT(-1) + CT(2) * af) / CT(8);
-    const CT a20 = (CT(1) + CT(2) * af) / CT(2);
+    const CT a60 = (CT(11) + xmul(CT(10), af)) / CT(16), a61 = (CT(15) + xmul(CT(34), af)) / CT(32);
+    const CT a62 = (CT(-3) + xmul(CT(6), af)) / CT(16), a63 = (CT(1) - xmul(CT(2), af)) / CT(32);
+    const CT a40 = (CT(5) + xmul(CT(6), af)) / CT(8), a41 = (CT(1) + xmul(CT(2), af)) / CT(2);
+    const CT a42 = (CT(-1) + xmul(CT(2), af)) / CT(8);
+    const CT a20 = (CT(1) + xmul(CT(2), af)) / CT(2);
+    const CT h61 = xmul(CT(0.5), a61), h62 = xmul(CT(0.5), a62), h63 = xmul(CT(0.5), a63);
+    const CT h41 = xmul(CT(0.5), a41), h42 = xmul(CT(0.5), a42), h21 = xmul(CT(0.5), a20);
     const int j0 = lane * LT;
     CT w[LT + 6];
 #pragma unroll
@@ -260,12 +269,12 @@ __device__ __forceinline__ void filter_rhs(const FT *f, int n, int lane, bool cy
         const int j = j0 + t;
         const CT c0 = w[t + 3];
         const CT s1 = w[t + 4] + w[t + 2], s2 = w[t + 5] + w[t + 1], s3 = w[t + 6] + w[t];
-        CT r = a60 * c0 + CT(0.5) * (a61 * s1 + a62 * s2 + a63 * s3);
+        CT r = xmul(a60, c0) + xmul(h61, s1) + xmul(h62, s2) + xmul(h63, s3);
         if (!cyclic) {
             const int dist = j < n - 1 - j ? j : n - 1 - j;
             if (dist == 0) r = c0;
-            else if (dist == 1) r = a20 * c0 + CT(0.5) * a20 * s1;
-            else if (dist == 2) r = a40 * c0 + CT(0.5) * (a41 * s1 + a42 * s2);
+            else if (dist == 1) r = xmul(a20, c0) + xmul(h21, s1);
+            else if (dist == 2) r = xmul(a40, c0) + xmul(h41, s1) + xmul(h42, s2);
         }
         d[t] = j < n ? r : CT(0);
     }

@@ -13,6 +13,7 @@
 #include <cstring>
 
 #include "context.h"
+#include "tile.cuh"
 
 namespace csb {
 
@@ -115,23 +116,6 @@ const DeviceTables *TableCache::get(int n, int scheme, int nstart, int nend, dou
 // ----------------------------------------------------------------------------
 // kernels
 // ----------------------------------------------------------------------------
-constexpr int kTileLines = 8;
-constexpr int kThreads = 256;
-
-// First point of line `fidx` (face index convention of
-// src/cuda/kernels/transforms.hpp: axis 0 k*let+j, axis 1 k*lxi+i, axis 2 j*lxi+i).
-template <int AXIS>
-__device__ __forceinline__ int64_t line_base(int64_t fidx, int lxi, int let) {
-    if (AXIS == 0) return fidx * lxi;
-    if (AXIS == 1) return (fidx / lxi) * (int64_t)lxi * let + fidx % lxi;
-    return fidx;
-}
-
-template <int AXIS>
-__device__ __forceinline__ int64_t line_stride(int lxi, int let) {
-    return AXIS == 0 ? 1 : (AXIS == 1 ? (int64_t)lxi : (int64_t)lxi * let);
-}
-
 // Stage the tile's lines into shared memory.
 template <int LT, int AXIS, typename T>
 __device__ __forceinline__ void load_tile(const T *__restrict__ in, T *sm, int64_t line0, int64_t F,
@@ -464,6 +448,15 @@ int cs_deriv_setup(cs_numerics *nm) {
         if (!nm->tables.get(n, kDeriv, nm->ndf[0][a], nm->ndf[1][a], 0.0)) return CS_ERR_UNSUPPORTED;
     }
     nm->setup_done = true;
+    return CS_OK;
+}
+
+int cs_interface_coeffs(double pbco[16], double pbci[16]) {
+    if (!pbco || !pbci) return set_error(CS_ERR_INVALID, "null argument");
+    Coeffs cf;
+    compute_interface_coeffs(cf);
+    std::memcpy(pbco, cf.pbco, sizeof cf.pbco);
+    std::memcpy(pbci, cf.pbci, sizeof cf.pbci);
     return CS_OK;
 }
 

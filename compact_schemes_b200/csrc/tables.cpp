@@ -17,53 +17,82 @@ namespace csb {
 // src/numerics_base.hpp:182-297).  Two coupled 8-point blocks form a 16-row
 // Pade system P f' = Q f; R = P~ P^-1 Q, where P~ is P without the rows'
 // coupling across the block interface.  Rows 8 and 9 of R hold the weights
-// a block applies to its neighbour's points (pbco, nearest point last) and to
-// its own points (pbci).  P^-1 Q is formed here by Gaussian elimination with
-// partial pivoting on [P | Q].
+// a block applies to its neighbour's points (pbco, nearest point first) and
+// to its own points (pbci).
+//
+// P^-1 is formed with the same Gauss-Jordan steps, in the same order, as
+// numerics_base::mtrxi (src/numerics_base.hpp:324-386), and the products in
+// the order of matmul_square (:388-398).  The weights multiply field values
+// in sums that cancel the field's mean, so for fields with a large mean (the
+// pressure part of a momentum flux) any last-bit difference in a weight is
+// amplified a few hundred times; reproducing the reference's operation order
+// makes the weights bit-identical to the reference's.
+static void invert_gauss_jordan(int n, const double *m, double *inv) {
+    std::vector<double> rx(m, m + n * n), temp(n);
+    std::vector<int> perm(n);
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int i = 0; i < n; ++i) {
+        // pivot column: largest |rx| in row i over columns i .. n-2
+        const int row0 = i * n + i, count = n - i - 1;
+        int best = 0;
+        double big = std::fabs(rx[row0]);
+        for (int k = 1; k < count; ++k) {
+            const double v = std::fabs(rx[row0 + k]);
+            if (v > big) { big = v; best = k; }
+        }
+        const int col = i + best;
+        if (col != i) {
+            std::swap(perm[col], perm[i]);
+            for (int r = 0; r < n; ++r) std::swap(rx[col + r * n], rx[i + r * n]);
+        }
+        const double piv_inv = 1.0 / rx[i + i * n];
+        for (int k = 0; k < n; ++k) temp[k] = rx[k + i * n];
+        for (int r = 0; r < n; ++r) {
+            const double f = piv_inv * rx[i + r * n];
+            for (int k = 0; k < n; ++k) rx[k + r * n] = rx[k + r * n] - f * temp[k];
+            rx[i + r * n] = f;
+        }
+        for (int k = 0; k < n; ++k) rx[k + i * n] = -piv_inv * temp[k];
+        rx[i + i * n] = piv_inv;
+    }
+    for (int r = 0; r < n; ++r)
+        for (int k = 0; k < n; ++k) inv[k + perm[r] * n] = rx[k + r * n];
+}
+
 void compute_interface_coeffs(Coeffs &cf) {
     const int n = 2 * kLmd;
-    double P[16][16] = {}, Q[16][16] = {}, M[16][32];
-    P[0][0] = 1.0; P[0][1] = kAlpha01;
-    P[1][0] = kAlpha10; P[1][1] = 1.0; P[1][2] = kAlpha10;
-    P[n - 1][n - 1] = 1.0; P[n - 1][n - 2] = kAlpha01;
-    P[n - 2][n - 1] = kAlpha10; P[n - 2][n - 2] = 1.0; P[n - 2][n - 3] = kAlpha10;
-    Q[0][0] = kAb00; Q[0][1] = kAb01; Q[0][2] = kAb02;
-    Q[1][0] = -kAb10; Q[1][2] = kAb10;
-    Q[n - 1][n - 1] = -kAb02; Q[n - 1][n - 2] = -kAb01; Q[n - 1][n - 3] = -kAb00;
-    Q[n - 2][n - 1] = kAb10; Q[n - 2][n - 3] = -kAb10;
+    std::vector<double> P(n * n, 0.0), Q(n * n, 0.0), Pi(n * n), T(n * n);
+    auto p = [&](int r, int c) -> double & { return P[r * n + c]; };
+    auto q = [&](int r, int c) -> double & { return Q[r * n + c]; };
+    p(0, 0) = 1.0; p(0, 1) = kAlpha01;
+    p(1, 0) = kAlpha10; p(1, 1) = 1.0; p(1, 2) = kAlpha10;
+    p(n - 1, n - 1) = 1.0; p(n - 1, n - 2) = kAlpha01;
+    p(n - 2, n - 1) = kAlpha10; p(n - 2, n - 2) = 1.0; p(n - 2, n - 3) = kAlpha10;
+    q(0, 0) = kAb00; q(0, 1) = kAb01; q(0, 2) = kAb02;
+    q(1, 0) = -kAb10; q(1, 2) = kAb10;
+    q(n - 1, n - 1) = -kAb02; q(n - 1, n - 2) = -kAb01; q(n - 1, n - 3) = -kAb00;
+    q(n - 2, n - 1) = kAb10; q(n - 2, n - 3) = -kAb10;
     for (int i = 2; i < n - 2; ++i) {
-        P[i][i - 1] = kAlpha; P[i][i] = 1.0; P[i][i + 1] = kAlpha;
-        Q[i][i - 2] = -kBb; Q[i][i - 1] = -kAa; Q[i][i + 1] = kAa; Q[i][i + 2] = kBb;
+        p(i, i - 1) = kAlpha; p(i, i) = 1.0; p(i, i + 1) = kAlpha;
+        q(i, i - 2) = -kBb; q(i, i - 1) = -kAa; q(i, i + 1) = kAa; q(i, i + 2) = kBb;
     }
-    for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) { M[i][j] = P[i][j]; M[i][n + j] = Q[i][j]; }
-    for (int col = 0; col < n; ++col) {
-        int piv = col;
-        for (int r = col + 1; r < n; ++r)
-            if (std::fabs(M[r][col]) > std::fabs(M[piv][col])) piv = r;
-        if (piv != col)
-            for (int j = 0; j < 2 * n; ++j) std::swap(M[col][j], M[piv][j]);
-        const double inv = 1.0 / M[col][col];
-        for (int j = 0; j < 2 * n; ++j) M[col][j] *= inv;
-        for (int r = 0; r < n; ++r) {
-            if (r == col || M[r][col] == 0.0) continue;
-            const double f = M[r][col];
-            for (int j = 0; j < 2 * n; ++j) M[r][j] -= f * M[col][j];
+    invert_gauss_jordan(n, P.data(), Pi.data());
+    // P~: drop the interface coupling of rows 6..9
+    p(6, 8) = 0.0; p(7, 8) = 0.0; p(7, 9) = 0.0;
+    p(9, 7) = 0.0; p(8, 7) = 0.0; p(8, 6) = 0.0;
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) {
+            double acc = 0.0;
+            for (int k = 0; k < n; ++k) acc += Pi[r * n + k] * Q[k * n + c];
+            T[r * n + c] = acc;
         }
-    }
-    // P~: drop the interface coupling of rows 6..9.
-    double Pt[16][16];
-    std::memcpy(Pt, P, sizeof P);
-    Pt[6][8] = 0.0; Pt[7][8] = 0.0; Pt[7][9] = 0.0;
-    Pt[9][7] = 0.0; Pt[8][7] = 0.0; Pt[8][6] = 0.0;
-    for (int row = 8; row <= 9; ++row) {
-        for (int col = 0; col < n; ++col) {
-            double s = 0.0;
-            for (int k = 0; k < n; ++k) s += Pt[row][k] * M[k][n + col];
-            if (col < kLmd) cf.pbco[(row - 8) * kLmd + kLmd - 1 - col] = s;
-            else cf.pbci[(row - 8) * kLmd + col - kLmd] = s;
+    for (int row = 8; row <= 9; ++row)
+        for (int c = 0; c < n; ++c) {
+            double acc = 0.0;
+            for (int k = 0; k < n; ++k) acc += P[row * n + k] * T[k * n + c];
+            if (c < kLmd) cf.pbco[(row - 8) * kLmd + kLmd - 1 - c] = acc;
+            else cf.pbci[(row - 8) * kLmd + c - kLmd] = acc;
         }
-    }
 }
 
 int chunk_length(int n) {

@@ -1,0 +1,103 @@
+"""Fused RHS / RK-stage solver over the C ABI (cs_solver_* in include/compact_b200.h).
+
+Replaces the per-stage driver sequence of the reference (driver/canard.cu:132-224):
+calc_time_step, calc_viscous_shear_stress, calc_fluxes, gcbc_go and the
+conserved-variable update, for one block held as a single rank on a uniform
+Cartesian grid.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+from . import check, lib, ptr, stream_ptr, BC_PERIODIC
+
+
+class SolverConfig(ctypes.Structure):
+    _fields_ = [("lxi", ctypes.c_int), ("let", ctypes.c_int), ("lze", ctypes.c_int),
+                ("nbc", ctypes.c_int * 3 * 2), ("viscous", ctypes.c_int), ("mu", ctypes.c_double),
+                ("umf", ctypes.c_double * 3), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+                ("dz", ctypes.c_double), ("cfl", ctypes.c_double), ("gcbc", ctypes.c_int),
+                ("use_graph", ctypes.c_int)]
+
+
+def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, dims=None,
+               nbc=None, gcbc=False):
+    """Taylor-Green box [0,2pi)^3 in CANARD units: mu = rho0 U0 L / Re with U0 = Mach."""
+    lxi, let, lze = dims if dims is not None else (n, n, n)
+    c = SolverConfig()
+    c.lxi, c.let, c.lze = lxi, let, lze
+    nbc = nbc if nbc is not None else [[BC_PERIODIC] * 3, [BC_PERIODIC] * 3]
+    for f in range(2):
+        for a in range(3):
+            c.nbc[f][a] = nbc[f][a]
+    c.viscous = int(viscous)
+    c.mu = mach / re
+    c.umf[:] = (0.0, 0.0, 0.0)
+    two_pi = 2.0 * math.pi
+    c.dx, c.dy, c.dz = two_pi / lxi, two_pi / let, two_pi / lze
+    c.cfl = cfl
+    c.gcbc = int(gcbc)
+    c.use_graph = int(use_graph)
+    return c
+
+
+class Solver:
+    def __init__(self, cfg: SolverConfig):
+        self.cfg = cfg
+        self._h = ctypes.c_void_p()
+        check(lib().cs_solver_create(ctypes.byref(self._h), ctypes.byref(cfg)))
+
+    @property
+    def lmx(self):
+        return self.cfg.lxi * self.cfg.let * self.cfg.lze
+
+    def close(self):
+        if self._h:
+            lib().cs_solver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def rhs(self, q, out, stream=None):
+        check(lib().cs_solver_rhs(self._h, ptr(q), ptr(out), stream_ptr(stream)))
+
+    def stage(self, k, qn, qin, qout, dt, stream=None):
+        check(lib().cs_solver_stage(self._h, k, ptr(qn), ptr(qin), ptr(qout), float(dt),
+                                    stream_ptr(stream)))
+
+    def step(self, q, dt=0.0, stream=None):
+        check(lib().cs_solver_step(self._h, ptr(q), float(dt), stream_ptr(stream)))
+
+    PASS_NAMES = ("grad_x", "grad_y", "grad_z", "flux_x", "flux_y", "flux_z_rk", "gcbc")
+
+    def profile_begin(self):
+        check(lib().cs_solver_profile_begin(self._h))
+
+    def profile_end(self):
+        """{pass name: (total ms, launches)} since profile_begin (synchronizes)."""
+        ms = (ctypes.c_double * 7)()
+        n = (ctypes.c_int * 7)()
+        check(lib().cs_solver_profile_end(self._h, ms, n))
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.PASS_NAMES)}
+
+    def step_host(self, q_in, q_out, dt=0.0, stream=None):
+        """One step on host buffers (pinned torch CPU tensors or any host memory)."""
+        check(lib().cs_solver_step_host(self._h, ctypes.c_void_p(q_in.data_ptr()),
+                                        ctypes.c_void_p(q_out.data_ptr()), float(dt),
+                                        stream_ptr(stream)))
+
+    def last_dt(self):
+        v = ctypes.c_double()
+        check(lib().cs_solver_last_dt(self._h, ctypes.byref(v)))
+        return v.value
+
+
+def tgv_init(q, dims, mach=0.1, noise=1e-4, seed=0, stream=None):
+    lxi, let, lze = dims
+    check(lib().cs_tgv_init(ptr(q), lxi, let, lze, float(mach), float(noise), int(seed),
+                            stream_ptr(stream)))

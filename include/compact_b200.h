@@ -73,6 +73,9 @@ int cs_numerics_destroy(cs_numerics *nm);
 /* numerics_base::deriv_setup (src/numerics_base.hpp:182-297): interface
  * weights pbco/pbci (copied to the device) and the line-solver tables. */
 int cs_deriv_setup(cs_numerics *nm);
+/* The same weights computed on the host without a numerics object (no device
+ * needed), bit-identical to the reference's deriv_setup. */
+int cs_interface_coeffs(double pbco[16], double pbci[16]);
 /* Host copies of pbco/pbci (16 each). */
 int cs_get_coeffs(const cs_numerics *nm, double pbco[16], double pbci[16]);
 /* ndf[face][axis] as in numerics_base::ndf (src/numerics_base.hpp:73-93). */
@@ -116,6 +119,66 @@ int cs_filter(cs_numerics *nm, int axis, const double *in, double *out, double a
  * scheme 0 = derivative (nstart/nend), 1 = filter (alpha_f). */
 int cs_line_tables(int n, int scheme, int nstart, int nend, double alpha_f, int meta[5],
                    double *tables, size_t tables_len);
+
+/* ---------------------------------------------------------------------------
+ * solver: fused RHS + RK stage on a uniform Cartesian grid
+ *
+ * Replaces, for one block held as a single rank, the per-stage sequence of
+ * the reference driver (driver/canard.cu:132-224): calc_time_step
+ * (src/physics_pc.hpp:229-256), calc_viscous_shear_stress (:151-227),
+ * calc_fluxes (:83-149), gcbc_go for non-reflective faces
+ * (src/gcbc.hpp:86-186) and the conserved-variable update that movef leaves
+ * empty (src/physics_base.hpp:147-150):
+ *     q^(k) = q^n - dt/(4-k) * J * de(q^(k-1)),  k = 0..3.
+ * Metrics are those of the uniform grid: xim = (dy dz, 0, 0),
+ * etm = (0, dx dz, 0), zem = (0, 0, dx dy), yaco = 1/(dx dy dz).
+ * ------------------------------------------------------------------------- */
+typedef struct cs_solver cs_solver;
+
+typedef struct {
+    int lxi, let, lze;  /* points per axis */
+    int nbc[2][3];      /* boundary code per face / axis (both faces of an axis periodic or both physical) */
+    int viscous;        /* physics<EnableViscous, T> */
+    double mu;          /* ssk: dynamic viscosity (constant) */
+    double umf[3];      /* physics_base::umf, moving-frame velocity */
+    double dx, dy, dz;  /* grid spacing */
+    double cfl;         /* CFL number when the time step is computed */
+    int gcbc;           /* apply non-reflective GCBC on x faces coded CS_BC_NON_REFLECTIVE */
+    int use_graph;      /* cs_solver_step replays a captured CUDA graph of the step */
+} cs_solver_config;
+
+int cs_solver_create(cs_solver **out, const cs_solver_config *cfg);
+int cs_solver_destroy(cs_solver *s);
+/* RHS de[m] = sum_a d/dxi_a F[m][a] of state q (physics::calc_viscous_shear_stress
+ * then physics::calc_fluxes, src/physics_pc.hpp:83-227), into rhs [5][lmx]. */
+int cs_solver_rhs(cs_solver *s, const double *q, double *rhs, void *stream);
+/* One RK stage k (0..3) with a given dt: qout = qn - dt/(4-k) J de(qin). */
+int cs_solver_stage(cs_solver *s, int k, const double *qn, const double *qin, double *qout,
+                    double dt, void *stream);
+/* One full RK step in place on the device state q [5][lmx]; dt <= 0 computes
+ * dt from q^n with the CFL formula of calc_time_step.  No host sync. */
+int cs_solver_step(cs_solver *s, double *q, double dt, void *stream);
+/* Same with host buffers: copies q_in_host [5][lmx] to a solver-owned device
+ * state, steps, copies the result to q_out_host and synchronizes the stream
+ * (pinned host memory makes the copies asynchronous DMA). */
+int cs_solver_step_host(cs_solver *s, const double *q_in_host, double *q_out_host, double dt,
+                        void *stream);
+/* dt used by the last step (synchronizing device-to-host copy). */
+int cs_solver_last_dt(cs_solver *s, double *dt);
+/* Device address of that dt (for stream-ordered readers). */
+int cs_solver_dt_device(cs_solver *s, double **dt_dev);
+/* Per-pass device timing of the eager step path (a graph step is not
+ * profiled): between begin and end every pass is bracketed by CUDA events on
+ * its stream; end synchronizes and returns the summed milliseconds and launch
+ * counts per pass kind: 0-2 gradient x/y/z, 3-5 flux x/y/z (z carries the RK
+ * update), 6 GCBC. */
+#define CS_PASS_KINDS 7
+int cs_solver_profile_begin(cs_solver *s);
+int cs_solver_profile_end(cs_solver *s, double ms[CS_PASS_KINDS], int launches[CS_PASS_KINDS]);
+/* Taylor-Green initial state on a periodic [0,2pi)^3 grid in CANARD units
+ * (no reference implementation: physics::init is empty, src/physics_pc.hpp:78-81). */
+int cs_tgv_init(double *q, int lxi, int let, int lze, double mach, double noise_amp,
+                uint64_t seed, void *stream);
 
 #ifdef __cplusplus
 }

@@ -62,14 +62,19 @@ def lib():
         L.or_viscous.restype = i32
         L.or_rhs.argtypes = [vp, vp, f64, Metrics, vp, i32, i32, i32, vp, i32, vp]
         L.or_rhs.restype = i32
+        L.or_rhs_scaled.argtypes = [vp, vp, f64, Metrics, vp, i32, i32, i32, vp, i32, vp, vp]
+        L.or_rhs_scaled.restype = i32
         L.or_gcbc_x.argtypes = [vp, vp, vp, vp, vp, vp, f64, vp, i32, i32, i32, vp]
         L.or_gcbc_x.restype = i32
         L.or_rk_step.argtypes = [vp, f64, Metrics, vp, i32, i32, i32, vp, i32, f64, f64, i32]
         L.or_rk_step.restype = f64
+        L.or_rk_stage.argtypes = [vp, vp, vp, i32, f64, f64, Metrics, vp, i32, i32, i32, vp, i32]
+        L.or_rk_stage.restype = f64
         L.or_tgv_init.argtypes = [vp, i32, i32, i32, f64, f64, ctypes.c_uint64]
         L.or_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.or_noise.restype = f64
         L.or_num_threads.restype = i32
+        L.or_set_reversed_solves.argtypes = [i32]
         _LIB = L
     return _LIB
 
@@ -198,16 +203,20 @@ def viscous(de, mu, metrics, dims, ndf):
     return tau, heat
 
 
-def rhs(q, mu, metrics, dims, ndf, viscous=True, umf=(0.0, 0.0, 0.0), drva_x=None):
+def rhs(q, mu, metrics, dims, ndf, viscous=True, umf=(0.0, 0.0, 0.0), drva_x=None,
+        with_scale=False):
+    """RHS de = sum_a d_a F[m][a]; with_scale also returns, per field, the max of
+    sum_a |d_a F[m][a]| (the size of the summed terms)."""
     lxi, let, lze = dims
     out = np.zeros_like(q)
     nd, ndp = _ip(ndf)
     u = np.asarray(umf, dtype=np.float64)
-    rc = lib().or_rhs(_p(q), _p(out), mu, metrics, _p(u), lxi, let, lze, ndp, int(viscous),
-                      _p(drva_x))
+    scale = np.zeros(5)
+    rc = lib().or_rhs_scaled(_p(q), _p(out), mu, metrics, _p(u), lxi, let, lze, ndp, int(viscous),
+                             _p(drva_x), _p(scale))
     if rc:
         raise ValueError("or_rhs failed")
-    return out
+    return (out, scale) if with_scale else out
 
 
 def gcbc_x(rhs_arr, drva_x, cm, q, sbcc, metrics, dims, nbc, umf=(0.0, 0.0, 0.0)):
@@ -234,6 +243,16 @@ def rk_step(q, mu, metrics, dims, nbc, viscous=True, dt=0.0, cfl=0.5, gcbc=False
     return dt
 
 
+def rk_stage(qn, qin, qout, k, dt, mu, metrics, dims, nbc, viscous=True, umf=(0.0, 0.0, 0.0)):
+    lxi, let, lze = dims
+    nb, nbp = _ip(nbc)
+    u = np.asarray(umf, dtype=np.float64)
+    r = lib().or_rk_stage(_p(qn), _p(qin), _p(qout), k, dt, mu, metrics, _p(u), lxi, let, lze, nbp,
+                          int(viscous))
+    if r < 0:
+        raise ValueError("or_rk_stage failed")
+
+
 def tgv_init(dims, mach=0.1, noise=1e-4, seed=0):
     lxi, let, lze = dims
     q = np.zeros(5 * lxi * let * lze)
@@ -243,6 +262,16 @@ def tgv_init(dims, mach=0.1, noise=1e-4, seed=0):
 
 def noise(seed, index):
     return lib().or_noise(seed, index)
+
+
+class reversed_solves:
+    """Context: the oracle solves its lines bottom-up (noise-floor measurement)."""
+
+    def __enter__(self):
+        lib().or_set_reversed_solves(1)
+
+    def __exit__(self, *exc):
+        lib().or_set_reversed_solves(0)
 
 
 def num_threads():

@@ -86,6 +86,21 @@ void thomas(int n, const double *a, const double *b, const double *c, const doub
     for (int i = n - 2; i >= 0; --i) x[i] = dp[i] - cp[i] * x[i + 1];
 }
 
+// When set, every derivative/filter line is solved bottom-up (Thomas on the
+// index-reversed system): exact-arithmetic identical, different rounding.
+// Tests use it to measure the FP64 noise floor of the scheme itself.
+int g_reversed = 0;
+
+void thomas_dir(int n, const double *a, const double *b, const double *c, const double *r, double *x) {
+    if (!g_reversed) { thomas(n, a, b, c, r, x); return; }
+    std::vector<double> ra(n), rb(n), rc(n), rr(n), rx(n);
+    for (int i = 0; i < n; ++i) {
+        ra[i] = c[n - 1 - i]; rb[i] = b[n - 1 - i]; rc[i] = a[n - 1 - i]; rr[i] = r[n - 1 - i];
+    }
+    thomas(n, ra.data(), rb.data(), rc.data(), rr.data(), rx.data());
+    for (int i = 0; i < n; ++i) x[i] = rx[n - 1 - i];
+}
+
 // Cyclic tridiagonal (a[0] couples x[n-1], c[n-1] couples x[0]) by the
 // Sherman-Morrison correction of a non-cyclic system.
 void thomas_cyclic(int n, const double *a, const double *b, const double *c, const double *r, double *x) {
@@ -104,29 +119,40 @@ void thomas_cyclic(int n, const double *a, const double *b, const double *c, con
     for (int i = 0; i < n; ++i) x[i] -= fact * z[i];
 }
 
-// Gauss-Jordan inverse with partial pivoting (row-major n x n).
-void invert(int n, const double *m, double *inv) {
-    std::vector<double> w(2 * n * n);
-    for (int i = 0; i < n; ++i)
-        for (int j = 0; j < 2 * n; ++j)
-            w[i * 2 * n + j] = j < n ? m[i * n + j] : (j - n == i ? 1.0 : 0.0);
-    for (int col = 0; col < n; ++col) {
-        int piv = col;
-        for (int r = col + 1; r < n; ++r)
-            if (std::fabs(w[r * 2 * n + col]) > std::fabs(w[piv * 2 * n + col])) piv = r;
-        if (piv != col)
-            for (int j = 0; j < 2 * n; ++j) std::swap(w[col * 2 * n + j], w[piv * 2 * n + j]);
-        double p = 1.0 / w[col * 2 * n + col];
-        for (int j = 0; j < 2 * n; ++j) w[col * 2 * n + j] *= p;
-        for (int r = 0; r < n; ++r) {
-            if (r == col) continue;
-            double f = w[r * 2 * n + col];
-            if (f == 0.0) continue;
-            for (int j = 0; j < 2 * n; ++j) w[r * 2 * n + j] -= f * w[col * 2 * n + j];
+// Matrix inverse by the steps of numerics_base::mtrxi / maxloc
+// (src/numerics_base.hpp:300-386): Gauss-Jordan elimination on the flattened
+// array rx[col + row*n], with the pivot column chosen by the largest |entry|
+// of row i among columns i .. n-2, columns swapped and a permutation kept.
+// The steps are kept identical (same operations in the same order) because
+// the interface weights it produces feed sums with strong cancellation, so
+// they must match the reference's to the last bit.
+void invert_like_reference(int n, const double *m, double *inv) {
+    std::vector<double> rx(m, m + n * n), temp(n);
+    std::vector<int> ipvt(n);
+    for (int i = 0; i < n; ++i) ipvt[i] = i;
+    for (int i = 0; i < n; ++i) {
+        const int loc = i * n + i, len = n - i - 1;
+        int imax = 0;
+        double dmax = std::fabs(rx[loc]);
+        for (int k = 1; k < len; ++k)
+            if (std::fabs(rx[loc + k]) > dmax) { dmax = std::fabs(rx[loc + k]); imax = k; }
+        const int mk = i + imax;
+        if (mk != i) {
+            std::swap(ipvt[mk], ipvt[i]);
+            for (int l = 0; l < n; ++l) std::swap(rx[mk + l * n], rx[i + l * n]);
         }
+        const double ra0 = 1.0 / rx[i + i * n];
+        for (int k = 0; k < n; ++k) temp[k] = rx[k + i * n];
+        for (int k = 0; k < n; ++k) {
+            const double ra1 = ra0 * rx[i + k * n];
+            for (int l = 0; l < n; ++l) rx[l + k * n] = rx[l + k * n] - ra1 * temp[l];
+            rx[i + k * n] = ra1;
+        }
+        for (int k = 0; k < n; ++k) rx[k + i * n] = -ra0 * temp[k];
+        rx[i + i * n] = ra0;
     }
-    for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) inv[i * n + j] = w[i * 2 * n + n + j];
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) inv[i + ipvt[j] * n] = rx[i + j * n];
 }
 
 // Rows of the compact derivative system for one line, restating
@@ -188,6 +214,8 @@ inline double jac(const or_metrics &m, int64_t i) { return m.yaco ? m.yaco[i] : 
 
 extern "C" {
 
+void or_set_reversed_solves(int on) { g_reversed = on ? 1 : 0; }
+
 int or_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();
@@ -217,7 +245,7 @@ void or_deriv_setup(double pbco[16], double pbci[16]) {
     p(1, 0) = kAlpha10; p(1, 1) = 1.0; p(1, 2) = kAlpha10;
     p(n - 2, n - 1) = kAlpha10; p(n - 2, n - 2) = 1.0; p(n - 2, n - 3) = kAlpha10;
     for (int i = 2; i < n - 2; ++i) { p(i, i) = 1.0; p(i, i - 1) = kAlpha; p(i, i + 1) = kAlpha; }
-    invert(n, P.data(), Pi.data());
+    invert_like_reference(n, P.data(), Pi.data());
     int i = n / 2 - 2;
     p(i, i + 2) = 0.0; p(i + 1, i + 2) = 0.0; p(i + 1, i + 3) = 0.0;
     i = n / 2 + 1;
@@ -274,7 +302,7 @@ int or_deriv_line(const double *f, double *x, int n, int nstart, int nend, const
     }
     std::vector<double> a(n), b(n), c(n), r(n);
     build_deriv_rows(f, n, nstart, nend, recv4, pbci, a.data(), b.data(), c.data(), r.data());
-    thomas(n, a.data(), b.data(), c.data(), r.data(), x);
+    thomas_dir(n, a.data(), b.data(), c.data(), r.data(), x);
     return 0;
 }
 
@@ -333,15 +361,15 @@ int or_filter_line(const double *f, double *x, int n, int nstart, int nend, doub
             a[i] = 0; c[i] = 0; r[i] = f[i];
         } else if (dist == 1) {
             a[i] = af; c[i] = af;
-            r[i] = a2[0] * at(i) + 0.5 * a2[1] * (at(i + 1) + at(i - 1));
+            r[i] = a2[0] * at(i) + (0.5 * a2[1]) * (at(i + 1) + at(i - 1));
         } else if (dist == 2) {
             a[i] = af; c[i] = af;
-            r[i] = a4[0] * at(i) + 0.5 * a4[1] * (at(i + 1) + at(i - 1)) +
-                   0.5 * a4[2] * (at(i + 2) + at(i - 2));
+            r[i] = a4[0] * at(i) + (0.5 * a4[1]) * (at(i + 1) + at(i - 1)) +
+                   (0.5 * a4[2]) * (at(i + 2) + at(i - 2));
         } else {
             a[i] = af; c[i] = af;
-            r[i] = a6[0] * at(i) + 0.5 * a6[1] * (at(i + 1) + at(i - 1)) +
-                   0.5 * a6[2] * (at(i + 2) + at(i - 2)) + 0.5 * a6[3] * (at(i + 3) + at(i - 3));
+            r[i] = a6[0] * at(i) + (0.5 * a6[1]) * (at(i + 1) + at(i - 1)) +
+                   (0.5 * a6[2]) * (at(i + 2) + at(i - 2)) + (0.5 * a6[3]) * (at(i + 3) + at(i - 3));
         }
     }
     if (cyclic) thomas_cyclic(n, a.data(), b.data(), c.data(), r.data(), x);
@@ -528,6 +556,12 @@ int or_viscous(const double *de, double mu, or_metrics m, int lxi, int let, int 
 // (src/physics_pc.hpp:83-227): de[m] = sum_a d_a F[m][a].
 int or_rhs(const double *q, double *rhs, double mu, or_metrics m, const double umf[3], int lxi,
            int let, int lze, const int ndf[2][3], int viscous, double *drva_x) {
+    return or_rhs_scaled(q, rhs, mu, m, umf, lxi, let, lze, ndf, viscous, drva_x, nullptr);
+}
+
+int or_rhs_scaled(const double *q, double *rhs, double mu, or_metrics m, const double umf[3],
+                  int lxi, int let, int lze, const int ndf[2][3], int viscous, double *drva_x,
+                  double *scale5) {
     ensure_coeffs();
     const int64_t n = (int64_t)lxi * let * lze;
     std::vector<double> de(5 * n), p(n), tau, heat;
@@ -546,7 +580,7 @@ int or_rhs(const double *q, double *rhs, double mu, or_metrics m, const double u
             etm[c * n + i] = metric(m.etm, m.c_etm, c, n, i);
             zem[c * n + i] = metric(m.zem, m.c_zem, c, n, i);
         }
-    std::vector<double> buf(15 * n), d(n);
+    std::vector<double> buf(15 * n), d(n), absum(scale5 ? n : 0);
     or_fluxes_pre(buf.data(), q, p.data(), de.data(), xim.data(), etm.data(), zem.data(),
                   viscous ? tau.data() : nullptr, viscous ? heat.data() : nullptr, umf, n);
     for (int v = 0; v < 5; ++v) {
@@ -563,6 +597,22 @@ int or_rhs(const double *q, double *rhs, double mu, or_metrics m, const double u
 #pragma omp parallel for
                 for (int64_t i = 0; i < n; ++i) r[i] += d[i];
             }
+            if (scale5) {
+                double *s = absum.data();
+                if (a == 0) {
+#pragma omp parallel for
+                    for (int64_t i = 0; i < n; ++i) s[i] = std::fabs(d[i]);
+                } else {
+#pragma omp parallel for
+                    for (int64_t i = 0; i < n; ++i) s[i] += std::fabs(d[i]);
+                }
+            }
+        }
+        if (scale5) {
+            double mx = 0.0;
+#pragma omp parallel for reduction(max : mx)
+            for (int64_t i = 0; i < n; ++i) mx = absum[i] > mx ? absum[i] : mx;
+            scale5[v] = mx;
         }
     }
     return 0;
@@ -697,6 +747,25 @@ double or_rk_step(double *q, double mu, or_metrics m, const double umf[3], int l
         }
     }
     std::memcpy(q, qk.data(), sizeof(double) * 5 * n);
+    return dt;
+}
+
+double or_rk_stage(const double *qn, const double *qin, double *qout, int k, double dt, double mu,
+                   or_metrics m, const double umf[3], int lxi, int let, int lze, const int nbc[2][3],
+                   int viscous) {
+    ensure_coeffs();
+    const int64_t n = (int64_t)lxi * let * lze;
+    int ndf[2][3];
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 3; ++a) ndf[f][a] = nbc[f][a] >= 35 ? 1 : 0;
+    std::vector<double> rhs(5 * n);
+    if (or_rhs(qin, rhs.data(), mu, m, umf, lxi, let, lze, ndf, viscous, nullptr)) return -1.0;
+    const double dtk = dt / (4 - k);
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) {
+        const double J = jac(m, i);
+        for (int v = 0; v < 5; ++v) qout[v * n + i] = qn[v * n + i] - dtk * J * rhs[v * n + i];
+    }
     return dt;
 }
 

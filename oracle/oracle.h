@@ -11,7 +11,7 @@
  * (src/cuda/kernels/physics.hpp:55-100).
  *
  * Parity pins: or_deriv_setup is checked against the reference's own
- * numerics_base::deriv_setup compiled from its sources (oracle/ref_build.sh);
+ * numerics_base::deriv_setup compiled from its sources (oracle/Makefile, target ref);
  * or_fluxes_pre and or_time_step against the reference's CPU twins in
  * tests/test_physics_serial.cu:41-163 and tests/test_physics.cu:57-117
  * compiled the same way; or_deriv against the known-answer linear-field test
@@ -96,6 +96,12 @@ int or_viscous(const double *de, double mu, or_metrics m, int lxi, int let, int 
 int or_rhs(const double *q, double *rhs, double mu, or_metrics m, const double umf[3],
            int lxi, int let, int lze, const int ndf[2][3], int viscous, double *drva_x);
 
+/* Same, also returning scale5[m] = max over points of sum_a |d_a F[m][a]|,
+ * the magnitude of the terms the RHS sums (the scale of its rounding error). */
+int or_rhs_scaled(const double *q, double *rhs, double mu, or_metrics m, const double umf[3],
+                  int lxi, int let, int lze, const int ndf[2][3], int viscous, double *drva_x,
+                  double *scale5);
+
 /* GCBC non-reflective correction of rhs on the x faces
  * (gcbc_go / gcbc_setup_kernel / gcbc_update_non_reflective_kernel,
  * src/gcbc.hpp:86-186, src/cuda/kernels/gcbc.hpp:251-454) with the reference
@@ -111,12 +117,22 @@ int or_gcbc_x(double *rhs, const double *drva_x, const double *cm, const double 
 double or_rk_step(double *q, double mu, or_metrics m, const double umf[3], int lxi, int let,
                   int lze, const int nbc[2][3], int viscous, double dt, double cfl, int gcbc);
 
+/* One stage k of that step: qout = qn - dt/(4-k) * J * rhs(qin). */
+double or_rk_stage(const double *qn, const double *qin, double *qout, int k, double dt, double mu,
+                   or_metrics m, const double umf[3], int lxi, int let, int lze, const int nbc[2][3],
+                   int viscous);
+
 /* Taylor-Green initial state on a periodic [0,2pi)^3 grid (CANARD units:
  * rho0 = 1, c_inf = 1, p0 = 1/gamma), density noise amp*U(-1,1) from the
  * counter-based generator or_noise. */
 void or_tgv_init(double *q, int lxi, int let, int lze, double mach, double noise_amp,
                  uint64_t seed);
 double or_noise(uint64_t seed, uint64_t index);
+
+/* Solve every line bottom-up instead of top-down (same mathematics, other
+ * rounding): the oracle against itself in this mode measures the FP64 noise
+ * floor of a quantity. */
+void or_set_reversed_solves(int on);
 
 int or_num_threads(void);
 

@@ -149,8 +149,8 @@ def test_coeffs_match_reference_golden(cuda):
     g = np.load(os.path.join(ROOT, "tests", "golden", "reference_pins.npz"))
     nm = make(cuda, (16, 16, 16), [[45] * 3, [45] * 3])
     pbco, pbci = nm.coeffs()
-    assert np.abs(np.array(pbco) - g["pbco"]).max() < 1e-15
-    assert np.abs(np.array(pbci) - g["pbci"]).max() < 1e-15
+    assert np.array_equal(np.array(pbco), g["pbco"])
+    assert np.array_equal(np.array(pbci), g["pbci"])
 
 
 @pytest.mark.parametrize("dims", [(64, 48, 40), (33, 17, 96), (7, 9, 256)])

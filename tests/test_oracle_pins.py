@@ -22,8 +22,9 @@ def gold():
 
 def test_deriv_setup_matches_reference(gold):
     pbco, pbci = O.deriv_setup()
-    assert np.abs(pbco - gold["pbco"]).max() < 1e-15
-    assert np.abs(pbci - gold["pbci"]).max() < 1e-15
+    # same steps as the reference's mtrxi/matmul_square: bit-identical
+    assert np.array_equal(pbco, gold["pbco"])
+    assert np.array_equal(pbci, gold["pbci"])
 
 
 def test_fluxes_pre_matches_reference_twin(gold):
