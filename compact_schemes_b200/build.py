@@ -11,6 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcompact_b200.so")
+EXTRA = []  # extra nvcc flags (-D knobs) for tuning builds
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
@@ -34,7 +35,7 @@ def _compile(src, verbose_regs=False):
     if (os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(path)
             and os.path.getmtime(obj) >= _headers_mtime() and not verbose_regs):
         return obj, ""
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *EXTRA, "-c", "-o", obj]
     if src.endswith(".cpp"):
         cmd += ["-x", "cu"]
     if verbose_regs:
@@ -46,7 +47,19 @@ def _compile(src, verbose_regs=False):
     return obj, r.stderr
 
 
-def build(verbose_regs=False, quiet=True):
+def build(verbose_regs=False, quiet=True, extra=None, build_dir=None, lib=None):
+    """Compile and link; `extra`/`build_dir`/`lib` build a variant elsewhere (tuning)."""
+    global EXTRA, BUILD, LIB
+    saved = (EXTRA, BUILD, LIB)
+    if extra is not None:
+        EXTRA, BUILD, LIB = list(extra), build_dir, lib
+    try:
+        return _build(verbose_regs, quiet)
+    finally:
+        EXTRA, BUILD, LIB = saved
+
+
+def _build(verbose_regs, quiet):
     os.makedirs(BUILD, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         results = list(ex.map(lambda s: _compile(s, verbose_regs), sources()))

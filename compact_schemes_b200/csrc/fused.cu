@@ -17,242 +17,9 @@
 #include <cstring>
 #include <vector>
 
-#include "context.h"
-#include "tile.cuh"
+#include "fused_kernels.cuh"
 
 namespace csb {
-
-struct Phys {
-    double M[3][3];  // metric rows xim, etm, zem (J^-1 grad xi_a)
-    double J;        // yaco
-    double mu;       // ssk (dynamic viscosity, constant)
-    double umf[3];   // moving-frame velocity
-    double rr1;      // sum of squared metric entries
-};
-
-struct RkParams {
-    double div;        // nkrk - k: stage coefficient dt / (nkrk - k)
-    double dt_fixed;   // > 0: use it; else CFL dt from dtacc
-    double cfl;
-    const unsigned long long *dtacc;  // two maxima as bit patterns of non-negative doubles
-    double *dt_out;
-};
-
-__device__ __forceinline__ double rk_dt(const RkParams &rk) {
-    if (rk.dt_fixed > 0.0) return rk.dt_fixed;
-    const double m1 = __longlong_as_double((long long)rk.dtacc[0]);
-    const double m2 = __longlong_as_double((long long)rk.dtacc[1]);
-    const double a = rk.cfl / m1, b = 0.5 / m2;
-    return a < b ? a : b;
-}
-
-// Primitive variables from the conserved state (CANARD units: T stored as
-// c^2 = gamma p / rho).
-struct Prim {
-    double rho, ri, u, v, w, p, T;
-};
-__device__ __forceinline__ Prim primitives(double q0, double q1, double q2, double q3, double q4) {
-    Prim s;
-    s.rho = q0;
-    s.ri = 1.0 / q0;
-    s.u = xmul(q1, s.ri);
-    s.v = xmul(q2, s.ri);
-    s.w = xmul(q3, s.ri);
-    s.p = xmul(kGamm1, q4 - xmul(0.5, xmul(q1, s.u) + xmul(q2, s.v) + xmul(q3, s.w)));
-    s.T = xmul(xmul(kGam, s.p), s.ri);
-    return s;
-}
-
-template <int LT>
-__device__ __forceinline__ double *field_line(double *sm, int field, int line) {
-    return sm + (field * kTileLines + line) * LineLayout<LT>::kSlot;
-}
-
-// Solve the derivative of nf fields of this warp's line held in shared memory
-// and overwrite them with the result.
-template <int LT, int NF>
-__device__ __forceinline__ void solve_fields(double *sm, int w, int lane, const DevTables<double> &tab,
-                                             int nstart, int nend, const Coeffs &cf) {
-#pragma unroll 1
-    for (int c = 0; c < NF; ++c) {
-        double *line = field_line<LT>(sm, c, w);
-        double d[1][LT];
-        deriv_rhs<LT, double, double>(line, tab.n, lane, nstart, nend, nullptr, cf, d[0]);
-        warp_solve<LT, 1, double>(tab, d, lane);
-        __syncwarp();
-#pragma unroll
-        for (int t = 0; t < LT; ++t)
-            if (lane * LT + t < tab.n) line[LineLayout<LT>::pos_ct(lane, t)] = d[0][t];
-    }
-}
-
-// ----------------------------------------------------------------------------
-// gradient pass: G[AXIS][c] = d/dxi_AXIS of (u, v, w, T)
-// ----------------------------------------------------------------------------
-template <int LT, int AXIS, bool DTRED>
-__global__ void __launch_bounds__(kThreads, 2)
-k_grad(const double *__restrict__ q, double *__restrict__ g, DevTables<double> tab, int lxi, int let,
-       int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf, Phys ph,
-       unsigned long long *__restrict__ dtacc) {
-    using L = LineLayout<LT>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sm = reinterpret_cast<double *>(smem_raw);
-    const int n = tab.n;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t line0 = (int64_t)blockIdx.x * kTileLines;
-    double m1 = 0.0, m2 = 0.0;
-    tile_for_each<AXIS, 2>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
-        const Prim s = primitives(__ldg(q + gi), __ldg(q + lmx + gi), __ldg(q + 2 * lmx + gi),
-                                  __ldg(q + 3 * lmx + gi), __ldg(q + 4 * lmx + gi));
-        const int pj = L::pos(j);
-        field_line<LT>(sm, 0, l)[pj] = s.u;
-        field_line<LT>(sm, 1, l)[pj] = s.v;
-        field_line<LT>(sm, 2, l)[pj] = s.w;
-        field_line<LT>(sm, 3, l)[pj] = s.T;
-        if (DTRED) {
-            // calc_time_step_kernel (src/cuda/kernels/physics.hpp:335-427)
-            const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
-            double rr2 = 0.0;
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-                rr2 += fabs(xmul(ph.M[a][0], uu) + xmul(ph.M[a][1], vv) + xmul(ph.M[a][2], ww));
-            const double ssi = fabs(ph.J);
-            const double v1 = xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi);
-            const double v2 = s.ri * ph.mu * ph.rr1 * ssi * ssi;
-            m1 = fmax(m1, v1);
-            m2 = fmax(m2, v2);
-        }
-    });
-    tile_sync<AXIS>();
-    const int64_t fidx = line0 + w;
-    if (fidx < F) solve_fields<LT, 4>(sm, w, lane, tab, nstart, nend, cf);
-    tile_sync<AXIS>();
-    tile_for_each<AXIS, 2>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
-        const int pj = L::pos(j);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) g[c * lmx + gi] = field_line<LT>(sm, c, l)[pj];
-    });
-    if (DTRED) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
-            m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
-        }
-        if (lane == 0) {
-            atomicMax(dtacc, (unsigned long long)__double_as_longlong(m1));
-            atomicMax(dtacc + 1, (unsigned long long)__double_as_longlong(m2));
-        }
-    }
-}
-
-// ----------------------------------------------------------------------------
-// flux pass
-// ----------------------------------------------------------------------------
-enum FluxMode { kWrite = 0, kAccum = 1, kAccumRk = 2, kWriteRk = 3 };
-
-// Flux components F[m][AXIS] at one point from the state and the gradients
-// (calc_fluxes_pre_compute_kernel<Visc>, src/cuda/kernels/physics.hpp:42-193,
-// with tau / heat flux of calc_viscous_shear_stress_final_kernel, :285-333).
-template <int AXIS, bool VISC>
-__device__ __forceinline__ void point_flux(const double *__restrict__ q, const double *__restrict__ g,
-                                           int64_t lmx, int64_t gi, const Phys &ph, double (&fl)[5]) {
-    const double q0 = __ldg(q + gi), q1 = __ldg(q + lmx + gi), q2 = __ldg(q + 2 * lmx + gi);
-    const double q3 = __ldg(q + 3 * lmx + gi), q4 = __ldg(q + 4 * lmx + gi);
-    double gr[12];
-    if (VISC) {
-#pragma unroll
-        for (int k = 0; k < 12; ++k) gr[k] = __ldg(g + k * lmx + gi);
-    }
-    const Prim s = primitives(q0, q1, q2, q3, q4);
-    const double *Ma = ph.M[AXIS];
-    const double ss = xmul(Ma[0], s.u + ph.umf[0]) + xmul(Ma[1], s.v + ph.umf[1]) + xmul(Ma[2], s.w + ph.umf[2]);
-    fl[0] = xmul(q0, ss);
-    fl[1] = xmul(q1, ss) + xmul(Ma[0], s.p);
-    fl[2] = xmul(q2, ss) + xmul(Ma[1], s.p);
-    fl[3] = xmul(q3, ss) + xmul(Ma[2], s.p);
-    fl[4] = xmul(q4 + s.p, ss) -
-            xmul(s.p, xmul(ph.umf[0], Ma[0]) + xmul(ph.umf[1], Ma[1]) + xmul(ph.umf[2], Ma[2]));
-    if (VISC) {
-        // physical gradients without the J factor: dc/dx_k = sum_b M[b][k] G[b][c]
-        double dx[4][3];
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                dx[c][k] = xmul(ph.M[0][k], gr[c]) + xmul(ph.M[1][k], gr[4 + c]) + xmul(ph.M[2][k], gr[8 + c]);
-        const double muj = xmul(ph.mu, ph.J);
-        const double kap = xmul(kGamm1Prndtli, muj);
-        const double div = xmul(2.0 / 3.0, dx[0][0] + dx[1][1] + dx[2][2]);
-        const double txx = xmul(muj, xmul(2.0, dx[0][0]) - div);
-        const double tyy = xmul(muj, xmul(2.0, dx[1][1]) - div);
-        const double tzz = xmul(muj, xmul(2.0, dx[2][2]) - div);
-        const double txy = xmul(muj, dx[1][0] + dx[0][1]);
-        const double tyz = xmul(muj, dx[2][1] + dx[1][2]);
-        const double tzx = xmul(muj, dx[0][2] + dx[2][0]);
-        const double hx = xmul(kap, dx[3][0]) + xmul(s.u, txx) + xmul(s.v, txy) + xmul(s.w, tzx);
-        const double hy = xmul(kap, dx[3][1]) + xmul(s.u, txy) + xmul(s.v, tyy) + xmul(s.w, tyz);
-        const double hz = xmul(kap, dx[3][2]) + xmul(s.u, tzx) + xmul(s.v, tyz) + xmul(s.w, tzz);
-        fl[1] -= xmul(Ma[0], txx) + xmul(Ma[1], txy) + xmul(Ma[2], tzx);
-        fl[2] -= xmul(Ma[0], txy) + xmul(Ma[1], tyy) + xmul(Ma[2], tyz);
-        fl[3] -= xmul(Ma[0], tzx) + xmul(Ma[1], tyz) + xmul(Ma[2], tzz);
-        fl[4] -= xmul(Ma[0], hx) + xmul(Ma[1], hy) + xmul(Ma[2], hz);
-    }
-}
-
-template <int LT, int AXIS, int MODE, bool VISC>
-__global__ void __launch_bounds__(kThreads, 2)
-k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__restrict__ rhs,
-       const double *__restrict__ qn, double *__restrict__ qout, double *__restrict__ drva,
-       DevTables<double> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend,
-       Coeffs cf, Phys ph, RkParams rk) {
-    using L = LineLayout<LT>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sm = reinterpret_cast<double *>(smem_raw);
-    const int n = tab.n;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t line0 = (int64_t)blockIdx.x * kTileLines;
-    tile_for_each<AXIS, 1>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
-        double fl[5];
-        point_flux<AXIS, VISC>(q, g, lmx, gi, ph, fl);
-        const int pj = L::pos(j);
-#pragma unroll
-        for (int m = 0; m < 5; ++m) field_line<LT>(sm, m, l)[pj] = fl[m];
-    });
-    tile_sync<AXIS>();
-    const int64_t fidx = line0 + w;
-    if (fidx < F) {
-        solve_fields<LT, 5>(sm, w, lane, tab, nstart, nend, cf);
-        if (drva) {
-            // line-end derivatives for the characteristic boundary closure
-            // (drva of deriv_kernel_2d, src/cuda/kernels/numerics_pc.hpp:237-248)
-            __syncwarp();
-            if (lane < 10) {
-                const int m = lane % 5, face = lane / 5;
-                drva[(int64_t)(face * 5 + m) * F + fidx] = field_line<LT>(sm, m, w)[L::pos(face ? n - 1 : 0)];
-            }
-        }
-    }
-    tile_sync<AXIS>();
-    double dtk = 0.0;
-    if (MODE >= kAccumRk) {
-        const double dt = rk_dt(rk);
-        dtk = xmul(dt / rk.div, ph.J);
-        if (rk.dt_out && blockIdx.x == 0 && threadIdx.x == 0) *rk.dt_out = dt;
-    }
-    tile_for_each<AXIS, 1>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
-        const int pj = L::pos(j);
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-            const double dfv = field_line<LT>(sm, m, l)[pj];
-            if (MODE == kWrite) rhs[m * lmx + gi] = dfv;
-            else if (MODE == kAccum) rhs[m * lmx + gi] += dfv;
-            else {
-                const double r = MODE == kAccumRk ? rhs[m * lmx + gi] + dfv : dfv;
-                qout[m * lmx + gi] = qn[m * lmx + gi] - xmul(dtk, r);
-            }
-        }
-    });
-}
 
 // ----------------------------------------------------------------------------
 // GCBC, non-reflective, x faces (gcbc_setup_kernel + gcbc_update_non_reflective_kernel,
@@ -349,18 +116,6 @@ __global__ void k_tgv(double *__restrict__ q, int lxi, int let, int64_t lmx, dou
     q[4 * lmx + idx] = p * kHamm1 + 0.5 * rho * (u * u + v * v + w * w);
 }
 
-// ----------------------------------------------------------------------------
-// host side
-// ----------------------------------------------------------------------------
-template <typename KernelT>
-static int set_smem(KernelT kern, size_t bytes) {
-    if (bytes > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
-    }
-    return CS_OK;
-}
-
 }  // namespace csb
 
 using namespace csb;
@@ -379,6 +134,7 @@ struct cs_solver {
     unsigned long long *dtacc = nullptr;
     double *dt_dev = nullptr;
     int64_t F[3] = {0, 0, 0};
+    int tile[2][3] = {{8, 8, 8}, {8, 8, 16}};  // lines per tile: [gradient|flux][axis]
     // optional per-pass event timing (eager path only)
     bool profiling = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof;
@@ -433,84 +189,40 @@ static int64_t fsize(const cs_dcomp &d, int a) {
 }
 static int llen(const cs_dcomp &d, int a) { return a == 0 ? d.lxi : (a == 1 ? d.let : d.lze); }
 
-template <int LT, int AXIS>
-static int launch_grad_lt(cs_solver *s, const double *q, bool dtred, cudaStream_t st) {
-    const size_t smem = (size_t)4 * kTileLines * LineLayout<LT>::kSlot * sizeof(double);
-    auto kern = dtred ? k_grad<LT, AXIS, true> : k_grad<LT, AXIS, false>;
-    if (int rc = set_smem(kern, smem)) return rc;
-    const int64_t F = s->F[AXIS];
-    const unsigned blocks = (unsigned)((F + kTileLines - 1) / kTileLines);
-    kern<<<blocks, kThreads, smem, st>>>(q, s->grad + (int64_t)AXIS * 4 * s->d.lmx, s->tab[AXIS]->t64,
-                                         s->d.lxi, s->d.let, s->d.lmx, F, s->ndf[0][AXIS],
-                                         s->ndf[1][AXIS], s->cf, s->ph, s->dtacc);
-    CSB_CUDA(cudaGetLastError());
-    return CS_OK;
-}
-
-template <int AXIS>
-static int launch_grad(cs_solver *s, const double *q, bool dtred, cudaStream_t st) {
-    switch (s->tab[AXIS]->lt) {
-        case 2: return launch_grad_lt<2, AXIS>(s, q, dtred, st);
-        case 4: return launch_grad_lt<4, AXIS>(s, q, dtred, st);
-        case 8: return launch_grad_lt<8, AXIS>(s, q, dtred, st);
-        case 16: return launch_grad_lt<16, AXIS>(s, q, dtred, st);
-        case 32: return launch_grad_lt<32, AXIS>(s, q, dtred, st);
-    }
-    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
+static PassArgs pass_args(cs_solver *s, int a, int kind) {
+    PassArgs p;
+    p.lmx = s->d.lmx;
+    p.lxi = s->d.lxi;
+    p.let = s->d.let;
+    p.F = s->F[a];
+    p.nstart = s->ndf[0][a];
+    p.nend = s->ndf[1][a];
+    p.tl = s->tile[kind][a];
+    p.viscous = s->cfg.viscous;
+    p.tab = s->tab[a];
+    p.cf = s->cf;
+    p.ph = s->ph;
+    p.grad = s->grad;
+    p.rhs = s->rhs;
+    p.dtacc = s->dtacc;
+    return p;
 }
 
 static int grad_pass(cs_solver *s, int a, const double *q, bool dtred, cudaStream_t st) {
     PassTimer pt(s, st, kPassGradX + a);
-    if (a == 0) return launch_grad<0>(s, q, dtred, st);
-    if (a == 1) return launch_grad<1>(s, q, dtred, st);
-    return launch_grad<2>(s, q, dtred, st);
-}
-
-template <int LT, int AXIS, int MODE>
-static int launch_flux_lt(cs_solver *s, const double *q, const double *qn, double *qout, double *drva,
-                          const RkParams &rk, cudaStream_t st) {
-    const size_t smem = (size_t)5 * kTileLines * LineLayout<LT>::kSlot * sizeof(double);
-    auto kern = s->cfg.viscous ? k_flux<LT, AXIS, MODE, true> : k_flux<LT, AXIS, MODE, false>;
-    if (int rc = set_smem(kern, smem)) return rc;
-    const int64_t F = s->F[AXIS];
-    const unsigned blocks = (unsigned)((F + kTileLines - 1) / kTileLines);
-    kern<<<blocks, kThreads, smem, st>>>(q, s->grad, s->rhs, qn, qout, drva, s->tab[AXIS]->t64, s->d.lxi,
-                                         s->d.let, s->d.lmx, F, s->ndf[0][AXIS], s->ndf[1][AXIS], s->cf,
-                                         s->ph, rk);
-    CSB_CUDA(cudaGetLastError());
-    return CS_OK;
-}
-
-template <int AXIS, int MODE>
-static int launch_flux_m(cs_solver *s, const double *q, const double *qn, double *qout, double *drva,
-                         const RkParams &rk, cudaStream_t st) {
-    switch (s->tab[AXIS]->lt) {
-        case 2: return launch_flux_lt<2, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
-        case 4: return launch_flux_lt<4, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
-        case 8: return launch_flux_lt<8, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
-        case 16: return launch_flux_lt<16, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
-        case 32: return launch_flux_lt<32, AXIS, MODE>(s, q, qn, qout, drva, rk, st);
-    }
-    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
-}
-
-template <int AXIS>
-static int launch_flux(cs_solver *s, int mode, const double *q, const double *qn, double *qout,
-                       double *drva, const RkParams &rk, cudaStream_t st) {
-    switch (mode) {
-        case kWrite: return launch_flux_m<AXIS, kWrite>(s, q, qn, qout, drva, rk, st);
-        case kAccum: return launch_flux_m<AXIS, kAccum>(s, q, qn, qout, drva, rk, st);
-        case kAccumRk: return launch_flux_m<AXIS, kAccumRk>(s, q, qn, qout, drva, rk, st);
-        default: return launch_flux_m<AXIS, kWriteRk>(s, q, qn, qout, drva, rk, st);
-    }
+    const PassArgs p = pass_args(s, a, 0);
+    if (a == 0) return launch_grad<0>(p, q, dtred, st);
+    if (a == 1) return launch_grad<1>(p, q, dtred, st);
+    return launch_grad<2>(p, q, dtred, st);
 }
 
 static int flux_pass(cs_solver *s, int a, int mode, const double *q, const double *qn, double *qout,
                      double *drva, const RkParams &rk, cudaStream_t st) {
     PassTimer pt(s, st, kPassFluxX + a);
-    if (a == 0) return launch_flux<0>(s, mode, q, qn, qout, drva, rk, st);
-    if (a == 1) return launch_flux<1>(s, mode, q, qn, qout, drva, rk, st);
-    return launch_flux<2>(s, mode, q, qn, qout, drva, rk, st);
+    const PassArgs p = pass_args(s, a, 1);
+    if (a == 0) return launch_flux<0>(p, mode, q, qn, qout, drva, rk, st);
+    if (a == 1) return launch_flux<1>(p, mode, q, qn, qout, drva, rk, st);
+    return launch_flux<2>(p, mode, q, qn, qout, drva, rk, st);
 }
 
 static bool gcbc_on(const cs_solver *s) {
@@ -610,6 +322,15 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         if (!s->tab[a]) { delete s; return CS_ERR_UNSUPPORTED; }
         s->active[a] = 1;
     }
+    for (int k = 0; k < 2; ++k)
+        for (int a = 0; a < 3; ++a) {
+            const int t = cfg->tile[k][a];
+            if (t != 0 && t != 8 && !(t == 16 && a > 0)) {
+                delete s;
+                return set_error(CS_ERR_INVALID, "tile[%d][%d] = %d: 8, or 16 for y/z, or 0", k, a, t);
+            }
+            if (t) s->tile[k][a] = t;
+        }
     compute_interface_coeffs(s->cf);
     const double hx = cfg->dx, hy = cfg->dy, hz = cfg->dz;
     std::memset(&s->ph, 0, sizeof s->ph);

@@ -1,0 +1,400 @@
+// fused_kernels.cuh -- device code of the fused RHS / RK-stage passes and
+// their launch templates (instantiated per axis in fused_axis{0,1,2}.cu).
+#pragma once
+
+#include <cmath>
+
+#include "context.h"
+#include "tile.cuh"
+
+// Tuning knobs (compile-time; defaults chosen by measurement on B200):
+// points per thread loaded together in the load phase of the gradient / flux
+// passes, points per thread in the store phase, minimum resident CTAs
+// (register cap) and the number of fields solved together by one warp.
+#ifndef CSB_GRAD_UNROLL
+#define CSB_GRAD_UNROLL 2
+#endif
+#ifndef CSB_FLUX_UNROLL
+#define CSB_FLUX_UNROLL 2
+#endif
+#ifndef CSB_STORE_UNROLL
+#define CSB_STORE_UNROLL 2
+#endif
+#ifndef CSB_GRAD_MINB
+#define CSB_GRAD_MINB 2
+#endif
+#ifndef CSB_FLUX_MINB
+#define CSB_FLUX_MINB 2
+#endif
+#ifndef CSB_SOLVE_GROUP
+#define CSB_SOLVE_GROUP 2
+#endif
+#ifndef CSB_RMW_CHUNK
+#define CSB_RMW_CHUNK 4     // points per chunk when only R is read back
+#endif
+#ifndef CSB_RMW_CHUNK_RK
+#define CSB_RMW_CHUNK_RK 2  // points per chunk when R and q^n are read (RK pass)
+#endif
+
+namespace csb {
+
+struct Phys {
+    double M[3][3];  // metric rows xim, etm, zem (J^-1 grad xi_a)
+    double J;        // yaco
+    double mu;       // ssk (dynamic viscosity, constant)
+    double umf[3];   // moving-frame velocity
+    double rr1;      // sum of squared metric entries
+};
+
+struct RkParams {
+    double div;        // nkrk - k: stage coefficient dt / (nkrk - k)
+    double dt_fixed;   // > 0: use it; else CFL dt from dtacc
+    double cfl;
+    const unsigned long long *dtacc;  // two maxima as bit patterns of non-negative doubles
+    double *dt_out;
+};
+
+__device__ __forceinline__ double rk_dt(const RkParams &rk) {
+    if (rk.dt_fixed > 0.0) return rk.dt_fixed;
+    const double m1 = __longlong_as_double((long long)rk.dtacc[0]);
+    const double m2 = __longlong_as_double((long long)rk.dtacc[1]);
+    const double a = rk.cfl / m1, b = 0.5 / m2;
+    return a < b ? a : b;
+}
+
+// Primitive variables from the conserved state (CANARD units: T stored as
+// c^2 = gamma p / rho).
+struct Prim {
+    double rho, ri, u, v, w, p, T;
+};
+__device__ __forceinline__ Prim primitives(double q0, double q1, double q2, double q3, double q4) {
+    Prim s;
+    s.rho = q0;
+    s.ri = 1.0 / q0;
+    s.u = xmul(q1, s.ri);
+    s.v = xmul(q2, s.ri);
+    s.w = xmul(q3, s.ri);
+    s.p = xmul(kGamm1, q4 - xmul(0.5, xmul(q1, s.u) + xmul(q2, s.v) + xmul(q3, s.w)));
+    s.T = xmul(xmul(kGam, s.p), s.ri);
+    return s;
+}
+
+template <int LT, int TL>
+__device__ __forceinline__ double *field_line(double *sm, int field, int line) {
+    return sm + (field * TL + line) * LineLayout<LT>::kSlot;
+}
+
+// Solve the derivative of NF fields of this warp's line held in shared memory
+// and overwrite them with the result; G fields share one warp_solve call
+// (their table loads and shuffles are interleaved).
+template <int LT, int TL, int NF, int G = CSB_SOLVE_GROUP>
+__device__ __forceinline__ void solve_fields(double *sm, int w, int lane, const DevTables<double> &tab,
+                                             int nstart, int nend, const Coeffs &cf) {
+#pragma unroll 1
+    for (int c0 = 0; c0 < NF; c0 += G) {
+        double d[G][LT];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            if (c0 + g < NF) deriv_rhs<LT, double, double>(field_line<LT, TL>(sm, c0 + g, w), tab.n, lane,
+                                                           nstart, nend, nullptr, cf, d[g]);
+            else {
+#pragma unroll
+                for (int t = 0; t < LT; ++t) d[g][t] = 0.0;
+            }
+        }
+        warp_solve<LT, G, double>(tab, d, lane);
+        __syncwarp();
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            if (c0 + g >= NF) continue;
+            double *line = field_line<LT, TL>(sm, c0 + g, w);
+#pragma unroll
+            for (int t = 0; t < LT; ++t)
+                if (lane * LT + t < tab.n) line[LineLayout<LT>::pos_ct(lane, t)] = d[g][t];
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// gradient pass: G[AXIS][c] = d/dxi_AXIS of (u, v, w, T)
+// ----------------------------------------------------------------------------
+template <int LT, int AXIS, int TL, bool DTRED>
+__global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_GRAD_MINB : 1)
+k_grad(const double *__restrict__ q, double *__restrict__ g, DevTables<double> tab, int lxi, int let,
+       int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf, Phys ph,
+       unsigned long long *__restrict__ dtacc) {
+    using L = LineLayout<LT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sm = reinterpret_cast<double *>(smem_raw);
+    const int n = tab.n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t line0 = (int64_t)blockIdx.x * TL;
+    double m1 = 0.0, m2 = 0.0;
+    tile_for_each<AXIS, TL, CSB_GRAD_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        const Prim s = primitives(__ldg(q + gi), __ldg(q + lmx + gi), __ldg(q + 2 * lmx + gi),
+                                  __ldg(q + 3 * lmx + gi), __ldg(q + 4 * lmx + gi));
+        const int pj = L::pos(j);
+        field_line<LT, TL>(sm, 0, l)[pj] = s.u;
+        field_line<LT, TL>(sm, 1, l)[pj] = s.v;
+        field_line<LT, TL>(sm, 2, l)[pj] = s.w;
+        field_line<LT, TL>(sm, 3, l)[pj] = s.T;
+        if (DTRED) {
+            // calc_time_step_kernel (src/cuda/kernels/physics.hpp:335-427)
+            const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
+            double rr2 = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                rr2 += fabs(xmul(ph.M[a][0], uu) + xmul(ph.M[a][1], vv) + xmul(ph.M[a][2], ww));
+            const double ssi = fabs(ph.J);
+            const double v1 = xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi);
+            const double v2 = s.ri * ph.mu * ph.rr1 * ssi * ssi;
+            m1 = fmax(m1, v1);
+            m2 = fmax(m2, v2);
+        }
+    });
+    tile_sync<AXIS, TL>();
+    const int64_t fidx = line0 + w;
+    if (fidx < F) solve_fields<LT, TL, 4>(sm, w, lane, tab, nstart, nend, cf);
+    tile_sync<AXIS, TL>();
+    tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        const int pj = L::pos(j);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) g[c * lmx + gi] = field_line<LT, TL>(sm, c, l)[pj];
+    });
+    if (DTRED) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+            m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+        }
+        if (lane == 0) {
+            atomicMax(dtacc, (unsigned long long)__double_as_longlong(m1));
+            atomicMax(dtacc + 1, (unsigned long long)__double_as_longlong(m2));
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// flux pass
+// ----------------------------------------------------------------------------
+enum FluxMode { kWrite = 0, kAccum = 1, kAccumRk = 2, kWriteRk = 3 };
+
+// Flux components F[m][AXIS] at one point from the state and the gradients
+// (calc_fluxes_pre_compute_kernel<Visc>, src/cuda/kernels/physics.hpp:42-193,
+// with tau / heat flux of calc_viscous_shear_stress_final_kernel, :285-333).
+template <int AXIS, bool VISC>
+__device__ __forceinline__ void point_flux(const double *__restrict__ q, const double *__restrict__ g,
+                                           int64_t lmx, int64_t gi, const Phys &ph, double (&fl)[5]) {
+    const double q0 = __ldg(q + gi), q1 = __ldg(q + lmx + gi), q2 = __ldg(q + 2 * lmx + gi);
+    const double q3 = __ldg(q + 3 * lmx + gi), q4 = __ldg(q + 4 * lmx + gi);
+    double gr[12];
+    if (VISC) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gr[k] = __ldg(g + k * lmx + gi);
+    }
+    const Prim s = primitives(q0, q1, q2, q3, q4);
+    const double *Ma = ph.M[AXIS];
+    const double ss = xmul(Ma[0], s.u + ph.umf[0]) + xmul(Ma[1], s.v + ph.umf[1]) + xmul(Ma[2], s.w + ph.umf[2]);
+    fl[0] = xmul(q0, ss);
+    fl[1] = xmul(q1, ss) + xmul(Ma[0], s.p);
+    fl[2] = xmul(q2, ss) + xmul(Ma[1], s.p);
+    fl[3] = xmul(q3, ss) + xmul(Ma[2], s.p);
+    fl[4] = xmul(q4 + s.p, ss) -
+            xmul(s.p, xmul(ph.umf[0], Ma[0]) + xmul(ph.umf[1], Ma[1]) + xmul(ph.umf[2], Ma[2]));
+    if (VISC) {
+        // physical gradients without the J factor: dc/dx_k = sum_b M[b][k] G[b][c]
+        double dx[4][3];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                dx[c][k] = xmul(ph.M[0][k], gr[c]) + xmul(ph.M[1][k], gr[4 + c]) + xmul(ph.M[2][k], gr[8 + c]);
+        const double muj = xmul(ph.mu, ph.J);
+        const double kap = xmul(kGamm1Prndtli, muj);
+        const double div = xmul(2.0 / 3.0, dx[0][0] + dx[1][1] + dx[2][2]);
+        const double txx = xmul(muj, xmul(2.0, dx[0][0]) - div);
+        const double tyy = xmul(muj, xmul(2.0, dx[1][1]) - div);
+        const double tzz = xmul(muj, xmul(2.0, dx[2][2]) - div);
+        const double txy = xmul(muj, dx[1][0] + dx[0][1]);
+        const double tyz = xmul(muj, dx[2][1] + dx[1][2]);
+        const double tzx = xmul(muj, dx[0][2] + dx[2][0]);
+        const double hx = xmul(kap, dx[3][0]) + xmul(s.u, txx) + xmul(s.v, txy) + xmul(s.w, tzx);
+        const double hy = xmul(kap, dx[3][1]) + xmul(s.u, txy) + xmul(s.v, tyy) + xmul(s.w, tyz);
+        const double hz = xmul(kap, dx[3][2]) + xmul(s.u, tzx) + xmul(s.v, tyz) + xmul(s.w, tzz);
+        fl[1] -= xmul(Ma[0], txx) + xmul(Ma[1], txy) + xmul(Ma[2], tzx);
+        fl[2] -= xmul(Ma[0], txy) + xmul(Ma[1], tyy) + xmul(Ma[2], tyz);
+        fl[3] -= xmul(Ma[0], tzx) + xmul(Ma[1], tyz) + xmul(Ma[2], tzz);
+        fl[4] -= xmul(Ma[0], hx) + xmul(Ma[1], hy) + xmul(Ma[2], hz);
+    }
+}
+
+template <int LT, int AXIS, int TL, int MODE, bool VISC>
+__global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_FLUX_MINB : 1)
+k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__restrict__ rhs,
+       const double *__restrict__ qn, double *__restrict__ qout, double *__restrict__ drva,
+       DevTables<double> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend,
+       Coeffs cf, Phys ph, RkParams rk) {
+    using L = LineLayout<LT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sm = reinterpret_cast<double *>(smem_raw);
+    const int n = tab.n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t line0 = (int64_t)blockIdx.x * TL;
+    tile_for_each<AXIS, TL, CSB_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        double fl[5];
+        point_flux<AXIS, VISC>(q, g, lmx, gi, ph, fl);
+        const int pj = L::pos(j);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) field_line<LT, TL>(sm, m, l)[pj] = fl[m];
+    });
+    tile_sync<AXIS, TL>();
+    const int64_t fidx = line0 + w;
+    if (fidx < F) {
+        solve_fields<LT, TL, 5>(sm, w, lane, tab, nstart, nend, cf);
+        if (drva) {
+            // line-end derivatives for the characteristic boundary closure
+            // (drva of deriv_kernel_2d, src/cuda/kernels/numerics_pc.hpp:237-248)
+            __syncwarp();
+            if (lane < 10) {
+                const int m = lane % 5, face = lane / 5;
+                drva[(int64_t)(face * 5 + m) * F + fidx] = field_line<LT, TL>(sm, m, w)[L::pos(face ? n - 1 : 0)];
+            }
+        }
+    }
+    tile_sync<AXIS, TL>();
+    double dtk = 0.0;
+    if (MODE >= kAccumRk) {
+        const double dt = rk_dt(rk);
+        dtk = xmul(dt / rk.div, ph.J);
+        if (rk.dt_out && blockIdx.x == 0 && threadIdx.x == 0) *rk.dt_out = dt;
+    }
+    if (MODE == kWrite) {
+        tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+            const int pj = L::pos(j);
+#pragma unroll
+            for (int m = 0; m < 5; ++m) rhs[m * lmx + gi] = field_line<LT, TL>(sm, m, l)[pj];
+        });
+    } else {
+        // read-modify-write: all loads of a chunk first
+        constexpr int P = MODE == kAccum ? CSB_RMW_CHUNK : CSB_RMW_CHUNK_RK;
+        double rv[P][5], qv[P][5];
+        tile_for_each_chunked<AXIS, TL, P>(
+            line0, F, n, lxi, let,
+            [&](int p, int l, int j, int64_t gi) {
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    rv[p][m] = MODE == kWriteRk ? 0.0 : rhs[m * lmx + gi];
+                    if (MODE >= kAccumRk) qv[p][m] = qn[m * lmx + gi];
+                }
+            },
+            [&](int p, int l, int j, int64_t gi) {
+                const int pj = L::pos(j);
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    const double dfv = field_line<LT, TL>(sm, m, l)[pj];
+                    if (MODE == kAccum) {
+                        rhs[m * lmx + gi] = rv[p][m] + dfv;
+                    } else {
+                        const double r = MODE == kAccumRk ? rv[p][m] + dfv : dfv;
+                        qout[m * lmx + gi] = qv[p][m] - xmul(dtk, r);
+                    }
+                }
+            });
+    }
+}
+
+
+// Everything one pass needs, independent of the solver object.
+struct PassArgs {
+    int64_t lmx;
+    int lxi, let;
+    int64_t F;
+    int nstart, nend;
+    int tl;        // lines per tile (8 or 16)
+    int viscous;
+    const DeviceTables *tab;
+    Coeffs cf;
+    Phys ph;
+    double *grad;  // [3][4][lmx]
+    double *rhs;   // [5][lmx]
+    unsigned long long *dtacc;
+};
+
+template <typename KernelT>
+inline int set_smem(KernelT kern, size_t bytes) {
+    if (bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+    }
+    return CS_OK;
+}
+
+template <int LT, int AXIS, int TL>
+int launch_grad_t(const PassArgs &a, const double *q, bool dtred, cudaStream_t st) {
+    const size_t smem = (size_t)4 * TL * LineLayout<LT>::kSlot * sizeof(double);
+    auto kern = dtred ? k_grad<LT, AXIS, TL, true> : k_grad<LT, AXIS, TL, false>;
+    if (int rc = set_smem(kern, smem)) return rc;
+    const unsigned blocks = (unsigned)((a.F + TL - 1) / TL);
+    kern<<<blocks, TL * 32, smem, st>>>(q, a.grad + (int64_t)AXIS * 4 * a.lmx, a.tab->t64, a.lxi, a.let,
+                                        a.lmx, a.F, a.nstart, a.nend, a.cf, a.ph, a.dtacc);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+template <int LT, int AXIS, int TL, int MODE>
+int launch_flux_t(const PassArgs &a, const double *q, const double *qn, double *qout, double *drva,
+                  const RkParams &rk, cudaStream_t st) {
+    const size_t smem = (size_t)5 * TL * LineLayout<LT>::kSlot * sizeof(double);
+    auto kern = a.viscous ? k_flux<LT, AXIS, TL, MODE, true> : k_flux<LT, AXIS, TL, MODE, false>;
+    if (int rc = set_smem(kern, smem)) return rc;
+    const unsigned blocks = (unsigned)((a.F + TL - 1) / TL);
+    kern<<<blocks, TL * 32, smem, st>>>(q, a.grad, a.rhs, qn, qout, drva, a.tab->t64, a.lxi, a.let, a.lmx,
+                                        a.F, a.nstart, a.nend, a.cf, a.ph, rk);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+template <int AXIS, int TL>
+int launch_grad_tl(const PassArgs &a, const double *q, bool dtred, cudaStream_t st) {
+    switch (a.tab->lt) {
+        case 2: return launch_grad_t<2, AXIS, TL>(a, q, dtred, st);
+        case 4: return launch_grad_t<4, AXIS, TL>(a, q, dtred, st);
+        case 8: return launch_grad_t<8, AXIS, TL>(a, q, dtred, st);
+        case 16: return launch_grad_t<16, AXIS, TL>(a, q, dtred, st);
+        case 32: return launch_grad_t<32, AXIS, TL>(a, q, dtred, st);
+    }
+    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
+}
+
+template <int AXIS, int TL, int MODE>
+int launch_flux_tm(const PassArgs &a, const double *q, const double *qn, double *qout, double *drva,
+                   const RkParams &rk, cudaStream_t st) {
+    switch (a.tab->lt) {
+        case 2: return launch_flux_t<2, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
+        case 4: return launch_flux_t<4, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
+        case 8: return launch_flux_t<8, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
+        case 16: return launch_flux_t<16, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
+        case 32: return launch_flux_t<32, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
+    }
+    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
+}
+
+template <int AXIS, int TL>
+int launch_flux_tl(const PassArgs &a, int mode, const double *q, const double *qn, double *qout,
+                   double *drva, const RkParams &rk, cudaStream_t st) {
+    switch (mode) {
+        case kWrite: return launch_flux_tm<AXIS, TL, kWrite>(a, q, qn, qout, drva, rk, st);
+        case kAccum: return launch_flux_tm<AXIS, TL, kAccum>(a, q, qn, qout, drva, rk, st);
+        case kAccumRk: return launch_flux_tm<AXIS, TL, kAccumRk>(a, q, qn, qout, drva, rk, st);
+        default: return launch_flux_tm<AXIS, TL, kWriteRk>(a, q, qn, qout, drva, rk, st);
+    }
+}
+
+// Per-axis entry points (fused_axis{0,1,2}.cu).
+template <int AXIS>
+int launch_grad(const PassArgs &a, const double *q, bool dtred, cudaStream_t st);
+template <int AXIS>
+int launch_flux(const PassArgs &a, int mode, const double *q, const double *qn, double *qout,
+                double *drva, const RkParams &rk, cudaStream_t st);
+
+}  // namespace csb

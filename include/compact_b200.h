@@ -145,6 +145,8 @@ typedef struct {
     double cfl;         /* CFL number when the time step is computed */
     int gcbc;           /* apply non-reflective GCBC on x faces coded CS_BC_NON_REFLECTIVE */
     int use_graph;      /* cs_solver_step replays a captured CUDA graph of the step */
+    int tile[2][3];     /* lines per tile of the [gradient|flux] pass along each axis:
+                           8, or 16 for y/z; 0 = default (16 for the z flux pass, else 8) */
 } cs_solver_config;
 
 int cs_solver_create(cs_solver **out, const cs_solver_config *cfg);
