@@ -26,6 +26,21 @@ def declare(L):
     L.cs_halo_exchange_self.argtypes = [vp, u32, vp]
     L.cs_filter.argtypes = [vp, i32, vp, vp, f64, Dcomp, vp]
     L.cs_line_tables.argtypes = [i32, i32, i32, i32, f64, vp, vp, sz]
+    L.cs_physics_create.argtypes = [pp, Dcomp, i32]
+    L.cs_physics_destroy.argtypes = [vp]
+    L.cs_physics_set_umf.argtypes = [vp, vp]
+    L.cs_physics_buffers.argtypes = [vp, pp, pp, pp, pp]
+    L.cs_calc_fluxes_pre.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+    L.cs_calc_fluxes.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, Dcomp, vp]
+    L.cs_calc_viscous_shear_stress.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, Dcomp, vp]
+    L.cs_calc_time_step.argtypes = [vp, vp, vp, vp, vp, vp, vp, f64, ctypes.POINTER(f64), sz, vp]
+    L.cs_gcbc_go.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, Dcomp, vp, vp]
+    L.cs_thermo.argtypes = [vp, vp, vp, sz, vp]
+    L.cs_rk_update.argtypes = [vp, vp, vp, f64, vp, sz, vp]
+    for name in ("cs_physics_create", "cs_physics_destroy", "cs_physics_set_umf", "cs_physics_buffers",
+                 "cs_calc_fluxes_pre", "cs_calc_fluxes", "cs_calc_viscous_shear_stress",
+                 "cs_calc_time_step", "cs_gcbc_go", "cs_thermo", "cs_rk_update"):
+        getattr(L, name).restype = i32
     from .solver import SolverConfig
     L.cs_solver_create.argtypes = [pp, ctypes.POINTER(SolverConfig)]
     L.cs_solver_destroy.argtypes = [vp]

@@ -121,6 +121,61 @@ int cs_line_tables(int n, int scheme, int nstart, int nend, double alpha_f, int 
                    double *tables, size_t tables_len);
 
 /* ---------------------------------------------------------------------------
+ * physics: the reference-shaped (unfused) path with per-point metric arrays
+ * ------------------------------------------------------------------------- */
+typedef struct cs_physics cs_physics;
+
+/* physics<EnableViscous, T>(t_dcomp) (src/physics_pc.hpp:62-72,
+ * src/physics_base.hpp:45-89): owns buffer / buffer_deriv [5][3][lmx],
+ * stress tensor [6][lmx] (xx, yy, zz, xy, yz, zx) and heat flux [3][lmx]. */
+int cs_physics_create(cs_physics **out, cs_dcomp d, int viscous);
+int cs_physics_destroy(cs_physics *ph);
+/* physics_base::umf (src/physics_base.hpp:155). */
+int cs_physics_set_umf(cs_physics *ph, const double umf[3]);
+/* Device pointers of the object's buffers (any may be NULL). */
+int cs_physics_buffers(cs_physics *ph, double **buffer, double **buffer_deriv, double **tau,
+                       double **heat);
+/* calc_fluxes_pre_compute (src/cuda/physics.hpp:41-62): the 15 contravariant
+ * fluxes into buffer, de[4] <- qa[4] + p.  de[1..3] hold u, v, w. */
+int cs_calc_fluxes_pre(cs_physics *ph, const double *qa, const double *p, double *de,
+                       const double *xim, const double *etm, const double *zem, void *stream);
+/* physics::calc_fluxes (src/physics_pc.hpp:83-149): pre-compute, interface
+ * sums and single-rank halo exchange, 15 compact derivatives,
+ * de[m] = sum_a d/dxi_a F[m][a].  Uses the numerics object's scratch. */
+int cs_calc_fluxes(cs_physics *ph, cs_numerics *nm, const double *qa, const double *p, double *de,
+                   const double *xim, const double *etm, const double *zem, cs_dcomp d,
+                   void *stream);
+/* physics::calc_viscous_shear_stress (src/physics_pc.hpp:151-227): gradients
+ * of de[1..4] = (u, v, w, T) by compact derivatives, chain rule through the
+ * metrics, stress tensor and energy flux into the object's buffers; like the
+ * reference it leaves de[0] = ssk and de[4] = 2/3 div u. */
+int cs_calc_viscous_shear_stress(cs_physics *ph, cs_numerics *nm, double *de, const double *ssk,
+                                 const double *xim, const double *etm, const double *zem,
+                                 const double *yaco, cs_dcomp d, void *stream);
+/* physics::calc_time_step (src/physics_pc.hpp:229-256): the CFL and viscous
+ * maxima on the device, dte = min(cfl / max1, 0.5 / max2) on the host
+ * (synchronizes the stream). */
+int cs_calc_time_step(cs_physics *ph, const double *xim, const double *etm, const double *zem,
+                      const double *de, const double *yaco, const double *ssk, double cfl,
+                      double *dte, size_t size, void *stream);
+/* Primitive recovery for the slot the reference driver leaves empty
+ * (driver/canard.cu:142-143): de0 = 1/rho, de1..3 = u, v, w,
+ * de4 = gamma p / rho (T in CANARD units, rho_inf = c_inf = 1), p. */
+int cs_thermo(const double *q, double *de, double *p, size_t n, void *stream);
+/* The update physics_base::movef leaves empty (src/physics_base.hpp:147-150):
+ * qout = qn - dtk * yaco * de (dtk = dt / (4 - k) for stage k). */
+int cs_rk_update(const double *qn, const double *de, const double *yaco, double dtk, double *qout,
+                 size_t n, void *stream);
+/* gcbc_go (src/gcbc.hpp:86-186) for non-reflective faces: characteristic
+ * projection of the numerics object's drva, incoming acoustic waves removed,
+ * de += sbcc * correction on the first 4 planes.  Faces coded periodic or
+ * interface are skipped; wall and curvilinear-interface codes return
+ * CS_ERR_UNSUPPORTED.  cm[axis]: [2][3][F] face normals. */
+int cs_gcbc_go(cs_numerics *nm, double *const cm[3], const double *qa, double *de, const double *p,
+               const double *yaco, const double *sbcc, const double umf[3], cs_dcomp d,
+               const int nbc[2][3], void *stream);
+
+/* ---------------------------------------------------------------------------
  * solver: fused RHS + RK stage on a uniform Cartesian grid
  *
  * Replaces, for one block held as a single rank, the per-stage sequence of

@@ -17,16 +17,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 TOL = 1e-12
 
 
-class _Raw:
-    def __init__(self, ptr, n):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
-                                         "version": 3}
-
-
-def device_view(ptr, n):
-    """torch view of n doubles of library-owned device memory."""
-    import torch
-    return torch.as_tensor(_Raw(ptr, n), device="cuda")
+from gpu_util import device_view  # noqa: E402
 
 
 def relerr(a, b):

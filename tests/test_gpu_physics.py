@@ -1,0 +1,152 @@
+"""GPU parity of the reference-shaped physics path (drop-in API) against the oracle
+and the reference's own CPU twins (tests/golden/reference_pins.npz)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_util import device_view
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MU = 0.1 / 1600
+
+
+def dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).to("cuda:0")
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(os.path.join(ROOT, "tests", "golden", "reference_pins.npz"))
+
+
+def test_fluxes_pre_against_reference_twin(cuda, gold):
+    """tests/test_physics_serial.cu restated: the flux pre-compute on the reference's
+    seeded inputs, vs its CPU twin (float) and vs the oracle (FP64, same operation order)."""
+    import compact_schemes_b200 as cs
+    g = {k: gold[k].astype(np.float64) for k in gold.files if k.startswith("flux_")}
+    n = g["flux_p"].size
+    ph = cs.physics((n, 1, 1), True)
+    ph.umf = g["flux_umf"]
+    _, _, tau, heat = ph.buffers()
+    import torch
+    device_view(tau, 6 * n).copy_(dev(g["flux_tau"]))
+    device_view(heat, 3 * n).copy_(dev(g["flux_heat"]))
+    de = dev(g["flux_de"])
+    ph.calc_fluxes_pre(dev(g["flux_qa"]), dev(g["flux_p"]), de, dev(g["flux_xim"]), dev(g["flux_etm"]),
+                       dev(g["flux_zem"]))
+    torch.cuda.synchronize()
+    b0, _, _, _ = ph.buffers()
+    got = device_view(b0, 15 * n).cpu().numpy()
+    assert rel(got, g["flux_buffer"]) < 1e-6          # reference twin is float32
+    ref, de_ref = O.fluxes_pre(g["flux_qa"], g["flux_p"], g["flux_de"], g["flux_xim"], g["flux_etm"],
+                               g["flux_zem"], g["flux_tau"], g["flux_heat"], g["flux_umf"])
+    assert np.array_equal(got, ref)                   # same operations, same order
+    assert np.array_equal(de.cpu().numpy(), de_ref)
+
+
+def test_time_step_against_reference_twin(cuda, gold):
+    """tests/test_physics.cu restated (single rank: the Allreduce is the identity)."""
+    import compact_schemes_b200 as cs
+    g = {k: gold[k].astype(np.float64) for k in gold.files if k.startswith("dt_")}
+    n = g["dt_yaco"].size
+    ph = cs.physics((n, 1, 1), False)
+    ph.umf = g["dt_umf"]
+    dte = ph.calc_time_step(dev(g["dt_xim"]), dev(g["dt_etm"]), dev(g["dt_zem"]), dev(g["dt_de"]),
+                            dev(g["dt_yaco"]), dev(g["dt_ssk"]), float(gold["dt_cfl"]), n)
+    assert abs(dte - float(gold["dt_result"])) / dte < 1e-6
+    ref = O.time_step(g["dt_xim"], g["dt_etm"], g["dt_zem"], g["dt_de"], g["dt_yaco"], g["dt_ssk"],
+                      g["dt_umf"], float(gold["dt_cfl"]))
+    assert dte == ref
+
+
+def metric_fields(dims, seed=3):
+    """Smooth, non-constant metric arrays (xim, etm, zem [3][n], yaco [n])."""
+    lxi, let, lze = dims
+    n = lxi * let * lze
+    i, j, k = np.meshgrid(np.arange(lxi), np.arange(let), np.arange(lze), indexing="ij")
+    ph = (2 * np.pi * (i / lxi + 2 * j / let + k / lze)).transpose(2, 1, 0).ravel()
+    h = 2 * np.pi / np.array(dims)
+    xim = np.zeros(3 * n); etm = np.zeros(3 * n); zem = np.zeros(3 * n)
+    xim[:n] = h[1] * h[2] * (1 + 0.05 * np.sin(ph)); xim[n:2 * n] = 0.01 * h[1] * h[2] * np.cos(ph)
+    etm[n:2 * n] = h[0] * h[2] * (1 + 0.05 * np.cos(ph)); etm[2 * n:] = 0.01 * h[0] * h[2] * np.sin(ph)
+    zem[2 * n:] = h[0] * h[1] * (1 - 0.05 * np.sin(ph)); zem[:n] = 0.01 * h[0] * h[1] * np.cos(2 * ph)
+    yaco = 1.0 / (h[0] * h[1] * h[2]) * (1 + 0.03 * np.cos(ph))
+    return xim, etm, zem, yaco
+
+
+@pytest.mark.parametrize("dims,periodic", [((32, 24, 20), True), ((24, 20, 16), False)])
+def test_viscous_and_fluxes_with_metric_arrays(cuda, dims, periodic):
+    """physics::calc_viscous_shear_stress + calc_fluxes with per-point metrics vs the oracle RHS."""
+    import torch
+    import compact_schemes_b200 as cs
+    b = cs.BC_PERIODIC if periodic else cs.BC_NON_REFLECTIVE
+    nbc = [[b] * 3, [b] * 3]
+    ndf = [[int(periodic)] * 3] * 2
+    n = int(np.prod(dims))
+    q = O.tgv_init(dims, 0.2, 1e-3, 5)
+    xim, etm, zem, yaco = metric_fields(dims)
+    m = O.field_metrics(xim, etm, zem, yaco)
+    ref, scale = O.rhs(q, MU, m, dims, ndf, with_scale=True)
+
+    nm = cs.numerics_pc(dims, nbc)
+    nm.deriv_setup()
+    ph = cs.physics(dims, True)
+    qd, X, E, Z, Y = dev(q), dev(xim), dev(etm), dev(zem), dev(yaco)
+    de = torch.zeros(5 * n, dtype=torch.float64, device="cuda")
+    p = torch.zeros(n, dtype=torch.float64, device="cuda")
+    ssk = torch.full((n,), MU, dtype=torch.float64, device="cuda")
+    cs.thermo(qd, de, p)
+    ph.calc_viscous_shear_stress(de, ssk, X, E, Z, Y, dims, None, nm)
+    cs.thermo(qd, de, p)   # the viscous call leaves de0 = ssk, de4 = 2/3 div (as the reference)
+    ph.calc_fluxes(qd, p, de, X, E, Z, dims, None, nm)
+    torch.cuda.synchronize()
+    got = de.cpu().numpy().reshape(5, n)
+    err = max(np.abs(got[i] - ref.reshape(5, n)[i]).max() / scale[i] for i in range(5))
+    assert err < 1e-12
+
+
+def test_gcbc_go_x_faces(cuda):
+    import torch
+    import compact_schemes_b200 as cs
+    dims = (40, 24, 16)
+    n = int(np.prod(dims))
+    nbc = [[10, 45, 45], [10, 45, 45]]
+    q = O.tgv_init(dims, 0.3, 1e-3, 1)
+    mm = O.uniform_metrics(*dims)
+    F = dims[1] * dims[2]
+    drva = np.zeros(10 * F)
+    ref = O.rhs(q, MU, mm, dims, [[0, 1, 1], [0, 1, 1]], drva_x=drva)
+    cm = np.zeros(6 * F); cm[:F] = 1.0; cm[3 * F:4 * F] = 1.0
+    sbcc = np.zeros(n); sbcc[::dims[0]] = 1.0 / mm.c_yaco; sbcc[dims[0] - 1::dims[0]] = 1.0 / mm.c_yaco
+    de_o, p_o = O.thermo(q)
+    rhs_o = ref.copy()
+    O.gcbc_x(rhs_o, drva, cm, q, sbcc, mm, dims, nbc)
+    # device: same RHS and drva, then gcbc_go
+    nm = cs.numerics_pc(dims, nbc)
+    nm.deriv_setup()
+    dp, _, _ = nm.buffers(0)
+    device_view(dp, 10 * F).copy_(dev(drva))
+    de = dev(ref)
+    yaco = torch.full((n,), mm.c_yaco, dtype=torch.float64, device="cuda")
+    cs.gcbc_go(nm, [dev(cm), None, None], dev(q), de, dev(p_o), yaco, dev(sbcc), (0.0, 0.0, 0.0), dims, nbc)
+    torch.cuda.synchronize()
+    got = de.cpu().numpy()
+    corr_o, corr_g = rhs_o - ref, got - ref
+    assert np.abs(corr_o).max() > 0
+    assert np.abs(corr_g - corr_o).max() / np.abs(corr_o).max() < 1e-12
+
+
+def test_dropin_cpp_demo_runs(cuda, tmp_path):
+    from test_dropin_build import build_demo
+    exe = build_demo(str(tmp_path / "dropin_demo"))
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
