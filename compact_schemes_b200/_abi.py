@@ -21,6 +21,8 @@ def declare(L):
     L.cs_get_ndf.argtypes = [vp, vp]
     L.cs_get_buffers.argtypes = [vp, i32, pp, pp, pp]
     L.cs_deriv.argtypes = [vp, i32, vp, vp, i32, i32, Dcomp, u32, u32, u32, i32, vp]
+    L.cs_deriv_noalloc.argtypes = [i32, vp, vp, i32, i32, Dcomp, vp]
+    L.cs_deriv_noalloc.restype = i32
     L.cs_deriv_f32.argtypes = [vp, i32, vp, vp, i32, i32, Dcomp, u32, u32, u32, i32, vp]
     L.cs_fill_buffers.argtypes = [vp, vp, i32, i32, i32, Dcomp, vp]
     L.cs_halo_exchange_self.argtypes = [vp, u32, vp]

@@ -92,6 +92,21 @@ int cs_get_buffers(cs_numerics *nm, int axis, double **drva, double **send, doub
  * variable `var`.  halo: CS_HALO_RECV or CS_HALO_SELF.  FP64. */
 int cs_deriv(cs_numerics *nm, int axis, const double *in, double *out, int nstart, int nend,
              cs_dcomp d, unsigned var, unsigned comp, unsigned slot, int halo, void *stream);
+/* The derivative of cs_deriv (FP64, deriv1d semantics: in and out are single
+ * fields) for callers that cannot let a library allocate device memory, e.g.
+ * applications that give all device memory to their own pool at start-up or
+ * that must not have cudaMalloc/cudaFree synchronize the device mid-loop.
+ * No counterpart in the reference.  It needs no numerics object and calls no
+ * allocation routine: its line-solver tables live in a file-scope device
+ * array of 64000 bytes (lines of at most 1024 points; longer lines return
+ * CS_ERR_UNSUPPORTED) that every GPU loading the library holds until exit.
+ * Interface faces (nstart/nend = 1) use the single-rank periodic closure; no
+ * line-end values are stored.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array and each rewrites it: calls that may
+ * overlap on the GPU (different streams, no ordering) race. */
+int cs_deriv_noalloc(int axis, const double *in, double *out, int nstart, int nend, cs_dcomp d,
+                     void *stream);
 /* Same for numerics_pc<float>: FP32 data and arithmetic. */
 int cs_deriv_f32(cs_numerics *nm, int axis, const float *in, float *out, int nstart, int nend,
                  cs_dcomp d, unsigned var, unsigned comp, unsigned slot, int halo, void *stream);
