@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--n", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-mixed", action="store_true")
     return p.parse_args()
 
 
@@ -285,6 +286,38 @@ def run_ours(args):
            "h2d_bytes_per_step": 5 * lmx * 8, "d2h_bytes_per_step": 5 * lmx * 8,
            "ms_per_step": te_ms / args.steps}
 
+    # --- mixed form: same workload and timing, error against the FP64 path -------
+    mixed = None
+    if not args.no_mixed:
+        sm = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, precision=1))
+        qm = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
+        cs.tgv_init(qm, dims, MACH, 1e-4, rank)
+        qp = qm.clone()
+        for _ in range(args.warmup):
+            sm.step(qm, 0.0)
+        barrier(world)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            sm.step(qm, 0.0)
+        g1.record(stream)
+        barrier(world)
+        tm_ms = max_over_ranks(g0.elapsed_time(g1), world)
+        # accuracy: W + K steps of each form from the same initial state
+        for _ in range(args.steps + args.warmup):
+            s.step(qp, 0.0)
+        torch.cuda.synchronize()
+        errs = [float((qm[i * lmx:(i + 1) * lmx] - qp[i * lmx:(i + 1) * lmx]).abs().max() /
+                      qp[i * lmx:(i + 1) * lmx].abs().max()) for i in range(5)]
+        mvalue = world * pts_stages_per_step * args.steps / (tm_ms * 1e-3) / 1e6
+        mixed = {"value": mvalue, "unit": UNIT, "ms_per_step": tm_ms / args.steps,
+                 "speedup_vs_plain": mvalue / value,
+                 "rel_err_vs_fp64_per_field": dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_E"], errs)),
+                 "steps_compared": args.steps + args.warmup,
+                 "arith": "FP32 fluxes/line solves; FP64 state, RK, thermo, RHS rows, refinement residual"}
+        sm.close()
+        del qm, qp
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, t, cores = cpu_oracle_stage_rate(n, stages=1)
@@ -303,7 +336,7 @@ def run_ours(args):
                            "rk": "4-stage, q^(k) = q^n - dt/(4-k) J R", "bc": "periodic (quasi-disjoint closure)",
                            "l2": "inputs larger than L2 (state 671 MB + gradients 1.6 GB), no flush",
                            "parallelism": "replicas" if world > 1 else "single GPU"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed,
                 "gpu_launches": 24 * args.steps, "clocks": clocks,
                 "passes": per_pass,
                 "stage_model": {"bytes_per_point": STAGE_BYTES, "ms_per_stage": stage_ms,

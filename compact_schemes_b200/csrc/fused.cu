@@ -17,7 +17,7 @@
 #include <cstring>
 #include <vector>
 
-#include "fused_kernels.cuh"
+#include "fused_mixed.cuh"
 
 namespace csb {
 
@@ -25,7 +25,8 @@ namespace csb {
 // GCBC, non-reflective, x faces (gcbc_setup_kernel + gcbc_update_non_reflective_kernel,
 // src/cuda/kernels/gcbc.hpp:251-454, reference defects fixed: see oracle/oracle.cpp)
 // ----------------------------------------------------------------------------
-__global__ void k_gcbc_x(double *__restrict__ rhs, const double *__restrict__ drva,
+template <typename RT>
+__global__ void k_gcbc_x(RT *__restrict__ rhs, const double *__restrict__ drva,
                          const double *__restrict__ q, int lxi, int64_t lmx, int64_t F, int face_mask,
                          Phys ph, double sb0, double sb1, double sb2, double sb3) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -85,7 +86,7 @@ __global__ void k_gcbc_x(double *__restrict__ rhs, const double *__restrict__ dr
         if (sb[ii] == 0.0) continue;
         const int64_t o = idx + (int64_t)ii * iq;
 #pragma unroll
-        for (int v = 0; v < 5; ++v) rhs[v * lmx + o] += xmul(sb[ii], dq[v]);
+        for (int v = 0; v < 5; ++v) rhs[v * lmx + o] = (RT)((double)rhs[v * lmx + o] + xmul(sb[ii], dq[v]));
     }
 }
 
@@ -131,6 +132,9 @@ struct cs_solver {
     int active[3] = {0, 0, 0};
     double *q1 = nullptr, *grad = nullptr, *rhs = nullptr, *drva = nullptr;
     double *qhost_dev = nullptr;  // device state for cs_solver_step_host
+    // mixed precision: FP32 deviation shadow, gradients and RHS
+    bool mixed = false;
+    float *sh32 = nullptr, *grad32 = nullptr, *rhs32 = nullptr;
     unsigned long long *dtacc = nullptr;
     double *dt_dev = nullptr;
     int64_t F[3] = {0, 0, 0};
@@ -225,6 +229,33 @@ static int flux_pass(cs_solver *s, int a, int mode, const double *q, const doubl
     return launch_flux<2>(p, mode, q, qn, qout, drva, rk, st);
 }
 
+static MixedArgs mixed_args(cs_solver *s, int a, int kind) {
+    MixedArgs m;
+    m.base = pass_args(s, a, kind);
+    m.shadow = s->sh32;
+    m.grad = s->grad32;
+    m.rhs = s->rhs32;
+    m.refine = s->cfg.refine;
+    return m;
+}
+
+static int grad_pass_mx(cs_solver *s, int a, const double *q, bool first, cudaStream_t st) {
+    PassTimer pt(s, st, kPassGradX + a);
+    const MixedArgs m = mixed_args(s, a, 0);
+    if (a == 0) return launch_grad_mx<0>(m, q, first, st);
+    if (a == 1) return launch_grad_mx<1>(m, q, first, st);
+    return launch_grad_mx<2>(m, q, first, st);
+}
+
+static int flux_pass_mx(cs_solver *s, int a, int mode, const double *qn, double *qout, bool shadow_out,
+                        double *drva, const RkParams &rk, cudaStream_t st) {
+    PassTimer pt(s, st, kPassFluxX + a);
+    const MixedArgs m = mixed_args(s, a, 1);
+    if (a == 0) return launch_flux_mx<0>(m, mode, qn, qout, shadow_out, drva, rk, st);
+    if (a == 1) return launch_flux_mx<1>(m, mode, qn, qout, shadow_out, drva, rk, st);
+    return launch_flux_mx<2>(m, mode, qn, qout, shadow_out, drva, rk, st);
+}
+
 static bool gcbc_on(const cs_solver *s) {
     return s->cfg.gcbc && s->active[0] &&
            (s->cfg.nbc[0][0] == CS_BC_NON_REFLECTIVE || s->cfg.nbc[1][0] == CS_BC_NON_REFLECTIVE);
@@ -261,13 +292,47 @@ static int run_stage(cs_solver *s, const double *qin, const double *qn, double *
             const int64_t F = s->F[0];
             int mask = (s->cfg.nbc[0][0] == CS_BC_NON_REFLECTIVE ? 1 : 0) |
                        (s->cfg.nbc[1][0] == CS_BC_NON_REFLECTIVE ? 2 : 0);
-            k_gcbc_x<<<(unsigned)((2 * F + 127) / 128), 128, 0, st>>>(s->rhs, s->drva, qin, s->d.lxi,
+            k_gcbc_x<double><<<(unsigned)((2 * F + 127) / 128), 128, 0, st>>>(s->rhs, s->drva, qin, s->d.lxi,
                                                                     s->d.lmx, F, mask, s->ph,
                                                                     1.0 / s->ph.J, 0.0, 0.0, 0.0);
             if (cudaGetLastError() != cudaSuccess) { s->rhs = saved_rhs; return set_error(CS_ERR_CUDA, "gcbc launch"); }
         }
     }
     s->rhs = saved_rhs;
+    return CS_OK;
+}
+
+// Mixed-precision stage.  The shadow of qin must be current unless
+// first_pass (stage 0), where the first gradient pass builds it from the FP64
+// state (and reduces the CFL maxima).
+static int run_stage_mx(cs_solver *s, const double *qin, const double *qn, double *qout, bool rhs_only,
+                        const RkParams *rk, bool first_pass, bool shadow_out, cudaStream_t st) {
+    int axes[3], na = 0;
+    for (int a = 0; a < 3; ++a)
+        if (s->active[a]) axes[na++] = a;
+    for (int i = 0; i < na; ++i)
+        if (s->cfg.viscous || (i == 0 && first_pass))
+            if (int rc = grad_pass_mx(s, axes[i], qin, first_pass && i == 0, st)) return rc;
+    RkParams none{};
+    for (int i = 0; i < na; ++i) {
+        const int a = axes[i];
+        int mode;
+        if (rhs_only) mode = i == 0 ? kWrite : kAccum;
+        else if (na == 1) mode = kWriteRk;
+        else mode = i == 0 ? kWrite : (i == na - 1 ? kAccumRk : kAccum);
+        double *drva = (a == 0 && gcbc_on(s)) ? s->drva : nullptr;
+        if (int rc = flux_pass_mx(s, a, mode, qn, qout, shadow_out, drva, rk ? *rk : none, st)) return rc;
+        if (drva && (mode == kWrite || mode == kAccum)) {
+            PassTimer pt(s, st, kPassGcbc);
+            const int64_t F = s->F[0];
+            const int mask = (s->cfg.nbc[0][0] == CS_BC_NON_REFLECTIVE ? 1 : 0) |
+                             (s->cfg.nbc[1][0] == CS_BC_NON_REFLECTIVE ? 2 : 0);
+            k_gcbc_x<float><<<(unsigned)((2 * F + 127) / 128), 128, 0, st>>>(s->rhs32, s->drva, qin, s->d.lxi,
+                                                                           s->d.lmx, F, mask, s->ph,
+                                                                           1.0 / s->ph.J, 0.0, 0.0, 0.0);
+            CSB_CUDA(cudaGetLastError());
+        }
+    }
     return CS_OK;
 }
 
@@ -283,6 +348,10 @@ static int run_step(cs_solver *s, double *q, double dt, cudaStream_t st) {
         rk.dt_out = k == 0 ? s->dt_dev : nullptr;
         const double *qin = k == 0 ? q : s->q1;
         double *qout = k == 3 ? q : s->q1;
+        if (s->mixed) {
+            if (int rc = run_stage_mx(s, qin, q, qout, false, &rk, k == 0, k < 3, st)) return rc;
+            continue;
+        }
         if (int rc = run_stage(s, qin, q, qout, nullptr, &rk, cfl && k == 0, st)) return rc;
     }
     return CS_OK;
@@ -322,6 +391,15 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         if (!s->tab[a]) { delete s; return CS_ERR_UNSUPPORTED; }
         s->active[a] = 1;
     }
+    if (cfg->precision != CS_PREC_FP64 && cfg->precision != CS_PREC_MIXED) {
+        delete s;
+        return set_error(CS_ERR_INVALID, "precision %d", cfg->precision);
+    }
+    int smem_max = 0, dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        smem_max = 227 * 1024;
+    const size_t elem = cfg->precision == CS_PREC_MIXED ? sizeof(float) : sizeof(double);
     for (int k = 0; k < 2; ++k)
         for (int a = 0; a < 3; ++a) {
             const int t = cfg->tile[k][a];
@@ -330,6 +408,26 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
                 return set_error(CS_ERR_INVALID, "tile[%d][%d] = %d: 8, or 16 for y/z, or 0", k, a, t);
             }
             if (t) s->tile[k][a] = t;
+            // the mixed form compiles 16-line tiles for the z axis only
+            if (cfg->precision == CS_PREC_MIXED && a == 1) s->tile[k][a] = 8;
+            if (!s->active[a]) continue;
+            // a tile holds 4 (gradient) or 5 (flux) staged fields of full lines
+            const size_t slot = (size_t)32 * s->tab[a]->lt + 1;
+            auto bytes = [&](int tl) { return (size_t)(k == 0 ? 4 : 5) * tl * slot * elem; };
+            if (bytes(s->tile[k][a]) > (size_t)smem_max) {
+                if (t) {
+                    delete s;
+                    return set_error(CS_ERR_UNSUPPORTED, "tile[%d][%d] = %d needs %zu bytes of shared memory", k, a,
+                                     t, bytes(t));
+                }
+                s->tile[k][a] = 8;
+            }
+            if (bytes(s->tile[k][a]) > (size_t)smem_max) {
+                delete s;
+                return set_error(CS_ERR_UNSUPPORTED,
+                                 "axis %d: lines of %d points do not fit the fused %s passes (%zu bytes of shared "
+                                 "memory per 8-line tile)", a, llen(s->d, a), elem == 8 ? "FP64" : "mixed", bytes(8));
+            }
         }
     compute_interface_coeffs(s->cf);
     const double hx = cfg->dx, hy = cfg->dy, hz = cfg->dz;
@@ -353,6 +451,17 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         return set_error(CS_ERR_ALLOC, "solver scratch allocation failed");
     }
     cudaMemset(s->grad, 0, 12 * lmx * sizeof(double));
+    if (cfg->precision == CS_PREC_MIXED) {
+        s->mixed = true;
+        const bool okm = cudaMalloc(&s->sh32, 5 * lmx * sizeof(float)) == cudaSuccess &&
+                         cudaMalloc(&s->grad32, 12 * lmx * sizeof(float)) == cudaSuccess &&
+                         cudaMalloc(&s->rhs32, 5 * lmx * sizeof(float)) == cudaSuccess;
+        if (!okm) {
+            cs_solver_destroy(s);
+            return set_error(CS_ERR_ALLOC, "mixed-precision scratch allocation failed");
+        }
+        cudaMemset(s->grad32, 0, 12 * lmx * sizeof(float));
+    }
     cudaMemset(s->dtacc, 0, 2 * sizeof(unsigned long long));
     cudaMemset(s->dt_dev, 0, sizeof(double));
     *out = s;
@@ -393,15 +502,30 @@ int cs_solver_destroy(cs_solver *s) {
     for (auto e : s->event_pool) cudaEventDestroy(e);
     if (s->graph) cudaGraphExecDestroy(s->graph);
     for (void *p : {(void *)s->q1, (void *)s->grad, (void *)s->rhs, (void *)s->drva, (void *)s->dtacc,
-                    (void *)s->dt_dev, (void *)s->qhost_dev})
+                    (void *)s->dt_dev, (void *)s->qhost_dev, (void *)s->sh32, (void *)s->grad32,
+                    (void *)s->rhs32})
         if (p) cudaFree(p);
     delete s;
     return CS_OK;
 }
 
+__global__ void k_widen(const float *__restrict__ a, double *__restrict__ b, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (double)a[i];
+}
+
 int cs_solver_rhs(cs_solver *s, const double *q, double *rhs, void *stream) {
     if (!s || !q || !rhs) return set_error(CS_ERR_INVALID, "null argument");
-    return run_stage(s, q, q, nullptr, rhs, nullptr, false, (cudaStream_t)stream);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (s->mixed) {
+        // build the shadow from q, assemble the FP32 RHS, widen it to FP64
+        if (int rc = run_stage_mx(s, q, q, nullptr, true, nullptr, true, false, st)) return rc;
+        const int64_t n = 5 * s->d.lmx;
+        k_widen<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s->rhs32, rhs, n);
+        CSB_CUDA(cudaGetLastError());
+        return CS_OK;
+    }
+    return run_stage(s, q, q, nullptr, rhs, nullptr, false, st);
 }
 
 int cs_solver_stage(cs_solver *s, int k, const double *qn, const double *qin, double *qout, double dt,
@@ -413,6 +537,7 @@ int cs_solver_stage(cs_solver *s, int k, const double *qn, const double *qin, do
     rk.dt_fixed = dt;
     rk.cfl = s->cfg.cfl;
     rk.dtacc = s->dtacc;
+    if (s->mixed) return run_stage_mx(s, qin, qn, qout, false, &rk, true, false, (cudaStream_t)stream);
     return run_stage(s, qin, qn, qout, nullptr, &rk, false, (cudaStream_t)stream);
 }
 

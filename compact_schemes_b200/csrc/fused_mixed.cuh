@@ -1,0 +1,390 @@
+// fused_mixed.cuh -- mixed-precision form of the fused RK-stage passes.
+//
+// FP64 master state q and FP64 RK accumulation; what the line solves consume
+// is FP32:
+//   * an FP32 "deviation shadow" of the stage state, (rho - rho0, u, v, w,
+//     p - p0) with the free-stream rho0 = 1, p0 = 1/gamma (CANARD units).  It
+//     is formed from q in FP64 (pressure and temperature recovered from total
+//     energy in FP64, where low-Mach cancellation needs it), so FP32 keeps its
+//     relative precision on the small deviations;
+//   * FP32 gradients of (u, v, w, T - T0) and an FP32 RHS accumulator R;
+//   * fluxes evaluated in FP64 from the shadow and rounded once to FP32 when
+//     staged.  They use the pressure deviation: with constant metrics the
+//     derivative of the constant part M*p0 is zero, so dropping it leaves the
+//     RHS unchanged while the FP32 derivative of a pressure-dominated flux
+//     keeps its precision;
+//   * line solves in FP32 on right-hand sides formed in FP64 (closure rows
+//     included), followed by one iterative-refinement sweep whose residual
+//     r - A x is formed in FP64.
+#pragma once
+
+#include "fused_kernels.cuh"
+
+namespace csb {
+
+constexpr double kRho0 = 1.0;
+constexpr double kP0 = 1.0 / kGam;
+constexpr double kT0 = kGam * kP0 / kRho0;  // = 1
+
+template <int LT, int TL>
+__device__ __forceinline__ float *field_line32(float *sm, int field, int line) {
+    return sm + (field * TL + line) * LineLayout<LT>::kSlot;
+}
+
+// Tridiagonal row coefficients of the derivative system (deriv_rows).
+__device__ __forceinline__ void deriv_row(int j, int n, int nstart, int nend, double &a, double &c) {
+    a = kAlpha;
+    c = kAlpha;
+    if (j == 0) { a = 0.0; c = nstart ? kAlpha : kAlpha01; }
+    else if (j == 1) { a = nstart ? kAlpha : kAlpha10; c = a; }
+    if (j == n - 1) { a = nend ? kAlpha : kAlpha01; c = 0.0; }
+    else if (j == n - 2) { a = nend ? kAlpha : kAlpha10; c = a; }
+}
+
+// FP32 solve of the derivative of NF fields (FP32 lines in shared memory)
+// with FP64 right-hand sides and, if refine, one FP64-residual refinement.
+template <int LT, int TL, int NF>
+__device__ __forceinline__ void solve_fields_mx(float *sm, int w, int lane, const DevTables<float> &tab,
+                                                int nstart, int nend, const Coeffs &cf, int refine) {
+    const int n = tab.n;
+    const int len = lane_len(lane, LT, tab.p, tab.last_len);
+#pragma unroll 1
+    for (int c = 0; c < NF; ++c) {
+        float *line = field_line32<LT, TL>(sm, c, w);
+        double r64[LT];
+        deriv_rhs<LT, double, float>(line, n, lane, nstart, nend, nullptr, cf, r64);
+        float x[1][LT];
+#pragma unroll
+        for (int t = 0; t < LT; ++t) x[0][t] = (float)r64[t];
+        warp_solve<LT, 1, float>(tab, x, lane);
+        if (refine) {
+            const float xm0 = __shfl_up_sync(0xffffffffu, x[0][LT - 1], 1);
+            const float xp0 = __shfl_down_sync(0xffffffffu, x[0][0], 1);
+            float e[1][LT];
+#pragma unroll
+            for (int t = 0; t < LT; ++t) {
+                const int j = lane * LT + t;
+                double a, cc;
+                deriv_row(j, n, nstart, nend, a, cc);
+                const double xm = t > 0 ? (double)x[0][t > 0 ? t - 1 : 0] : (double)xm0;
+                double xp = (double)xp0;
+#pragma unroll
+                for (int u = 0; u + 1 < LT; ++u)
+                    if (u == t && t + 1 < len) xp = (double)x[0][u + 1];
+                const double res = r64[t] - (a * xm + (double)x[0][t] + cc * xp);
+                e[0][t] = j < n ? (float)res : 0.0f;
+            }
+            warp_solve<LT, 1, float>(tab, e, lane);
+#pragma unroll
+            for (int t = 0; t < LT; ++t) x[0][t] += e[0][t];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < LT; ++t)
+            if (lane * LT + t < n) line[LineLayout<LT>::pos_ct(lane, t)] = x[0][t];
+    }
+}
+
+// FP32 shadow values of one point from the FP64 state (thermo in FP64).
+__device__ __forceinline__ void shadow_from_q(double q0, double q1, double q2, double q3, double q4,
+                                              float (&sh)[5], Prim &s) {
+    s = primitives(q0, q1, q2, q3, q4);
+    sh[0] = (float)(q0 - kRho0);
+    sh[1] = (float)s.u;
+    sh[2] = (float)s.v;
+    sh[3] = (float)s.w;
+    sh[4] = (float)(s.p - kP0);
+}
+
+// T - T0 from the shadow deviations, in FP64: with gamma p0 = T0 rho0,
+// T - T0 = (gamma dp - T0 drho) / (rho0 + drho), free of cancellation.
+__device__ __forceinline__ double temp_dev(float dr, float dp) {
+    return ((double)kGam * (double)dp - kT0 * (double)dr) / (kRho0 + (double)dr);
+}
+
+// ----------------------------------------------------------------------------
+// gradient pass (FIRST: reads the FP64 state, writes the shadow, reduces CFL)
+// ----------------------------------------------------------------------------
+template <int LT, int AXIS, int TL, bool FIRST>
+__global__ void __launch_bounds__(TL * 32, TL == 8 ? 2 : 1)
+k_grad_mx(const double *__restrict__ q, float *__restrict__ sh, float *__restrict__ g,
+          DevTables<float> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf,
+          Phys ph, unsigned long long *__restrict__ dtacc, int refine) {
+    using L = LineLayout<LT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *sm = reinterpret_cast<float *>(smem_raw);
+    const int n = tab.n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t line0 = (int64_t)blockIdx.x * TL;
+    double m1 = 0.0, m2 = 0.0;
+    tile_for_each<AXIS, TL, CSB_GRAD_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        float u, v, wv, tp;
+        if (FIRST) {
+            float s5[5];
+            Prim s;
+            shadow_from_q(__ldg(q + gi), __ldg(q + lmx + gi), __ldg(q + 2 * lmx + gi), __ldg(q + 3 * lmx + gi),
+                          __ldg(q + 4 * lmx + gi), s5, s);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) sh[k * lmx + gi] = s5[k];
+            u = s5[1];
+            v = s5[2];
+            wv = s5[3];
+            tp = (float)temp_dev(s5[0], s5[4]);
+            const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
+            double rr2 = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                rr2 += fabs(xmul(ph.M[a][0], uu) + xmul(ph.M[a][1], vv) + xmul(ph.M[a][2], ww));
+            const double ssi = fabs(ph.J);
+            m1 = fmax(m1, xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi));
+            m2 = fmax(m2, s.ri * ph.mu * ph.rr1 * ssi * ssi);
+        } else {
+            const float dr = __ldg(sh + gi), dp = __ldg(sh + 4 * lmx + gi);
+            u = __ldg(sh + lmx + gi);
+            v = __ldg(sh + 2 * lmx + gi);
+            wv = __ldg(sh + 3 * lmx + gi);
+            tp = (float)temp_dev(dr, dp);
+        }
+        const int pj = L::pos(j);
+        field_line32<LT, TL>(sm, 0, l)[pj] = u;
+        field_line32<LT, TL>(sm, 1, l)[pj] = v;
+        field_line32<LT, TL>(sm, 2, l)[pj] = wv;
+        field_line32<LT, TL>(sm, 3, l)[pj] = tp;
+    });
+    tile_sync<AXIS, TL>();
+    if (line0 + w < F) solve_fields_mx<LT, TL, 4>(sm, w, lane, tab, nstart, nend, cf, refine);
+    tile_sync<AXIS, TL>();
+    tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        const int pj = L::pos(j);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) g[c * lmx + gi] = field_line32<LT, TL>(sm, c, l)[pj];
+    });
+    if (FIRST) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+            m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+        }
+        if (lane == 0) {
+            atomicMax(dtacc, (unsigned long long)__double_as_longlong(m1));
+            atomicMax(dtacc + 1, (unsigned long long)__double_as_longlong(m2));
+        }
+    }
+}
+
+// Flux components F[m][AXIS], evaluated in FP64 from the FP32 shadow and FP32
+// gradients (the inputs are exact in FP64, so only the final rounding to FP32
+// when staging adds error).
+template <int AXIS, bool VISC>
+__device__ __forceinline__ void point_flux_mx(const float *__restrict__ sh, const float *__restrict__ g,
+                                              int64_t lmx, int64_t gi, const Phys &ph, float (&flo)[5]) {
+    const double dr = __ldg(sh + gi), u = __ldg(sh + lmx + gi), v = __ldg(sh + 2 * lmx + gi);
+    const double wv = __ldg(sh + 3 * lmx + gi), dp = __ldg(sh + 4 * lmx + gi);
+    double gr[12];
+    if (VISC) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gr[k] = (double)__ldg(g + k * lmx + gi);
+    }
+    const double rho = kRho0 + dr;
+    const double *Ma = ph.M[AXIS];
+    const double ss = Ma[0] * (u + ph.umf[0]) + Ma[1] * (v + ph.umf[1]) + Ma[2] * (wv + ph.umf[2]);
+    // rho*H = gamma/(gamma-1) p + rho |u|^2 / 2 with p = p0 + dp
+    const double rH = kGam * kHamm1 * (kP0 + dp) + 0.5 * rho * (u * u + v * v + wv * wv);
+    double fl[5];
+    fl[0] = rho * ss;
+    fl[1] = rho * u * ss + Ma[0] * dp;
+    fl[2] = rho * v * ss + Ma[1] * dp;
+    fl[3] = rho * wv * ss + Ma[2] * dp;
+    fl[4] = rH * ss - dp * (ph.umf[0] * Ma[0] + ph.umf[1] * Ma[1] + ph.umf[2] * Ma[2]);
+    if (VISC) {
+        double dx[4][3];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) dx[c][k] = ph.M[0][k] * gr[c] + ph.M[1][k] * gr[4 + c] + ph.M[2][k] * gr[8 + c];
+        const double muj = ph.mu * ph.J;
+        const double kap = kGamm1Prndtli * muj;
+        const double div = 2.0 / 3.0 * (dx[0][0] + dx[1][1] + dx[2][2]);
+        const double txx = muj * (2.0 * dx[0][0] - div), tyy = muj * (2.0 * dx[1][1] - div);
+        const double tzz = muj * (2.0 * dx[2][2] - div);
+        const double txy = muj * (dx[1][0] + dx[0][1]), tyz = muj * (dx[2][1] + dx[1][2]);
+        const double tzx = muj * (dx[0][2] + dx[2][0]);
+        const double hx = kap * dx[3][0] + u * txx + v * txy + wv * tzx;
+        const double hy = kap * dx[3][1] + u * txy + v * tyy + wv * tyz;
+        const double hz = kap * dx[3][2] + u * tzx + v * tyz + wv * tzz;
+        fl[1] -= Ma[0] * txx + Ma[1] * txy + Ma[2] * tzx;
+        fl[2] -= Ma[0] * txy + Ma[1] * tyy + Ma[2] * tyz;
+        fl[3] -= Ma[0] * tzx + Ma[1] * tyz + Ma[2] * tzz;
+        fl[4] -= Ma[0] * hx + Ma[1] * hy + Ma[2] * hz;
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m) flo[m] = (float)fl[m];
+}
+
+template <int LT, int AXIS, int TL, int MODE, bool VISC, bool SHADOW_OUT>
+__global__ void __launch_bounds__(TL * 32, TL == 8 ? 2 : 1)
+k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__restrict__ rhs,
+          const double *__restrict__ qn, double *__restrict__ qout, float *__restrict__ sh_out,
+          double *__restrict__ drva, DevTables<float> tab, int lxi, int let, int64_t lmx, int64_t F,
+          int nstart, int nend, Coeffs cf, Phys ph, RkParams rk, int refine) {
+    using L = LineLayout<LT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *sm = reinterpret_cast<float *>(smem_raw);
+    const int n = tab.n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t line0 = (int64_t)blockIdx.x * TL;
+    tile_for_each<AXIS, TL, CSB_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        float fl[5];
+        point_flux_mx<AXIS, VISC>(sh, g, lmx, gi, ph, fl);
+        const int pj = L::pos(j);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) field_line32<LT, TL>(sm, m, l)[pj] = fl[m];
+    });
+    tile_sync<AXIS, TL>();
+    const int64_t fidx = line0 + w;
+    if (fidx < F) {
+        solve_fields_mx<LT, TL, 5>(sm, w, lane, tab, nstart, nend, cf, refine);
+        if (drva) {
+            __syncwarp();
+            if (lane < 10) {
+                const int m = lane % 5, face = lane / 5;
+                drva[(int64_t)(face * 5 + m) * F + fidx] =
+                    (double)field_line32<LT, TL>(sm, m, w)[L::pos(face ? n - 1 : 0)];
+            }
+        }
+    }
+    tile_sync<AXIS, TL>();
+    double dtk = 0.0;
+    if (MODE >= kAccumRk) {
+        const double dt = rk_dt(rk);
+        dtk = xmul(dt / rk.div, ph.J);
+        if (rk.dt_out && blockIdx.x == 0 && threadIdx.x == 0) *rk.dt_out = dt;
+    }
+    if (MODE == kWrite) {
+        tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+            const int pj = L::pos(j);
+#pragma unroll
+            for (int m = 0; m < 5; ++m) rhs[m * lmx + gi] = field_line32<LT, TL>(sm, m, l)[pj];
+        });
+    } else {
+        constexpr int P = MODE == kAccum ? CSB_RMW_CHUNK : CSB_RMW_CHUNK_RK;
+        float rv[P][5];
+        double qv[P][5];
+        tile_for_each_chunked<AXIS, TL, P>(
+            line0, F, n, lxi, let,
+            [&](int p, int l, int j, int64_t gi) {
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    rv[p][m] = MODE == kWriteRk ? 0.0f : rhs[m * lmx + gi];
+                    if (MODE >= kAccumRk) qv[p][m] = qn[m * lmx + gi];
+                }
+            },
+            [&](int p, int l, int j, int64_t gi) {
+                const int pj = L::pos(j);
+                if (MODE == kAccum) {
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) rhs[m * lmx + gi] = rv[p][m] + field_line32<LT, TL>(sm, m, l)[pj];
+                } else {
+                    double qo[5];
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) {
+                        const double r = (double)rv[p][m] + (double)field_line32<LT, TL>(sm, m, l)[pj];
+                        qo[m] = qv[p][m] - xmul(dtk, r);
+                        qout[m * lmx + gi] = qo[m];
+                    }
+                    if (SHADOW_OUT) {
+                        float s5[5];
+                        Prim s;
+                        shadow_from_q(qo[0], qo[1], qo[2], qo[3], qo[4], s5, s);
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) sh_out[m * lmx + gi] = s5[m];
+                    }
+                }
+            });
+    }
+}
+
+struct MixedArgs {
+    PassArgs base;
+    float *shadow;  // [5][lmx]
+    float *grad;    // [3][4][lmx]
+    float *rhs;     // [5][lmx]
+    int refine;
+};
+
+template <int LT, int AXIS, int TL>
+int launch_grad_mx_t(const MixedArgs &a, const double *q, bool first, cudaStream_t st) {
+    const size_t smem = (size_t)4 * TL * LineLayout<LT>::kSlot * sizeof(float);
+    auto kern = first ? k_grad_mx<LT, AXIS, TL, true> : k_grad_mx<LT, AXIS, TL, false>;
+    if (int rc = set_smem(kern, smem)) return rc;
+    const PassArgs &b = a.base;
+    const unsigned blocks = (unsigned)((b.F + TL - 1) / TL);
+    kern<<<blocks, TL * 32, smem, st>>>(q, a.shadow, a.grad + (int64_t)AXIS * 4 * b.lmx, b.tab->t32, b.lxi,
+                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, b.dtacc, a.refine);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+template <int LT, int AXIS, int TL, int MODE>
+int launch_flux_mx_t(const MixedArgs &a, const double *qn, double *qout, bool shadow_out, double *drva,
+                     const RkParams &rk, cudaStream_t st) {
+    const size_t smem = (size_t)5 * TL * LineLayout<LT>::kSlot * sizeof(float);
+    const PassArgs &b = a.base;
+    // the shadow is written only by the RK modes
+    constexpr bool kRk = MODE >= kAccumRk;
+    auto kern = b.viscous ? (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, true, kRk>
+                                               : k_flux_mx<LT, AXIS, TL, MODE, true, false>)
+                          : (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, false, kRk>
+                                               : k_flux_mx<LT, AXIS, TL, MODE, false, false>);
+    if (int rc = set_smem(kern, smem)) return rc;
+    const unsigned blocks = (unsigned)((b.F + TL - 1) / TL);
+    kern<<<blocks, TL * 32, smem, st>>>(a.shadow, a.grad, a.rhs, qn, qout, a.shadow, drva, b.tab->t32, b.lxi,
+                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, rk, a.refine);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+template <int AXIS, int TL>
+int launch_grad_mx_tl(const MixedArgs &a, const double *q, bool first, cudaStream_t st) {
+    switch (a.base.tab->lt) {
+        case 2: return launch_grad_mx_t<2, AXIS, TL>(a, q, first, st);
+        case 4: return launch_grad_mx_t<4, AXIS, TL>(a, q, first, st);
+        case 8: return launch_grad_mx_t<8, AXIS, TL>(a, q, first, st);
+        case 16: return launch_grad_mx_t<16, AXIS, TL>(a, q, first, st);
+        case 32: return launch_grad_mx_t<32, AXIS, TL>(a, q, first, st);
+    }
+    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
+}
+
+template <int AXIS, int TL, int MODE>
+int launch_flux_mx_tm(const MixedArgs &a, const double *qn, double *qout, bool shadow_out, double *drva,
+                      const RkParams &rk, cudaStream_t st) {
+    switch (a.base.tab->lt) {
+        case 2: return launch_flux_mx_t<2, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
+        case 4: return launch_flux_mx_t<4, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
+        case 8: return launch_flux_mx_t<8, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
+        case 16: return launch_flux_mx_t<16, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
+        case 32: return launch_flux_mx_t<32, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
+    }
+    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
+}
+
+template <int AXIS, int TL>
+int launch_flux_mx_tl(const MixedArgs &a, int mode, const double *qn, double *qout, bool shadow_out,
+                      double *drva, const RkParams &rk, cudaStream_t st) {
+    switch (mode) {
+        case kWrite: return launch_flux_mx_tm<AXIS, TL, kWrite>(a, qn, qout, shadow_out, drva, rk, st);
+        case kAccum: return launch_flux_mx_tm<AXIS, TL, kAccum>(a, qn, qout, shadow_out, drva, rk, st);
+        case kAccumRk: return launch_flux_mx_tm<AXIS, TL, kAccumRk>(a, qn, qout, shadow_out, drva, rk, st);
+        default: return launch_flux_mx_tm<AXIS, TL, kWriteRk>(a, qn, qout, shadow_out, drva, rk, st);
+    }
+}
+
+// Per-axis entry points (fused_mixed_axis{0,1,2}.cu).
+template <int AXIS>
+int launch_grad_mx(const MixedArgs &a, const double *q, bool first, cudaStream_t st);
+template <int AXIS>
+int launch_flux_mx(const MixedArgs &a, int mode, const double *qn, double *qout, bool shadow_out,
+                   double *drva, const RkParams &rk, cudaStream_t st);
+
+}  // namespace csb

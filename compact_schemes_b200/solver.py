@@ -18,11 +18,16 @@ class SolverConfig(ctypes.Structure):
                 ("nbc", ctypes.c_int * 3 * 2), ("viscous", ctypes.c_int), ("mu", ctypes.c_double),
                 ("umf", ctypes.c_double * 3), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
                 ("dz", ctypes.c_double), ("cfl", ctypes.c_double), ("gcbc", ctypes.c_int),
-                ("use_graph", ctypes.c_int), ("tile", ctypes.c_int * 3 * 2)]
+                ("use_graph", ctypes.c_int), ("tile", ctypes.c_int * 3 * 2),
+                ("precision", ctypes.c_int), ("refine", ctypes.c_int)]
+
+
+PREC_FP64 = 0
+PREC_MIXED = 1
 
 
 def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, dims=None,
-               nbc=None, gcbc=False, tile=None):
+               nbc=None, gcbc=False, tile=None, precision=PREC_FP64, refine=1):
     """Taylor-Green box [0,2pi)^3 in CANARD units: mu = rho0 U0 L / Re with U0 = Mach."""
     lxi, let, lze = dims if dims is not None else (n, n, n)
     c = SolverConfig()
@@ -39,6 +44,8 @@ def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, di
     c.cfl = cfl
     c.gcbc = int(gcbc)
     c.use_graph = int(use_graph)
+    c.precision = int(precision)
+    c.refine = int(refine)
     if tile is not None:
         for k in range(2):
             for a in range(3):

@@ -205,6 +205,11 @@ int cs_gcbc_go(cs_numerics *nm, double *const cm[3], const double *qa, double *d
  * ------------------------------------------------------------------------- */
 typedef struct cs_solver cs_solver;
 
+#define CS_PREC_FP64 0  /* plain FP64 */
+#define CS_PREC_MIXED 1 /* FP32 fluxes and line solves (FP64 right-hand sides and one
+                           FP64-residual refinement sweep), FP64 state, RK accumulation
+                           and thermodynamics */
+
 typedef struct {
     int lxi, let, lze;  /* points per axis */
     int nbc[2][3];      /* boundary code per face / axis (both faces of an axis periodic or both physical) */
@@ -216,7 +221,11 @@ typedef struct {
     int gcbc;           /* apply non-reflective GCBC on x faces coded CS_BC_NON_REFLECTIVE */
     int use_graph;      /* cs_solver_step replays a captured CUDA graph of the step */
     int tile[2][3];     /* lines per tile of the [gradient|flux] pass along each axis:
-                           8, or 16 for y/z; 0 = default (16 for the z flux pass, else 8) */
+                           8, or 16 for y/z; 0 = default (16 for the z flux pass, else 8);
+                           tiles that do not fit shared memory fall back to 8; the mixed
+                           form uses 8 for y */
+    int precision;      /* CS_PREC_FP64 or CS_PREC_MIXED */
+    int refine;         /* mixed: one FP64-residual refinement sweep per line solve (1) or none (0) */
 } cs_solver_config;
 
 int cs_solver_create(cs_solver **out, const cs_solver_config *cfg);

@@ -1,0 +1,90 @@
+"""Mixed-precision form: FP32 fluxes and line solves (FP64 right-hand sides and
+one FP64-residual refinement sweep), FP64 state, RK accumulation and
+thermodynamics.
+
+Target (north star): relative state error <= 1e-6 per field after 100 RK steps
+against the FP64 path.  Relative error of a field f: max|f - f64| / max|f64|.
+rho*w starts at exactly zero in the Taylor-Green state, so its relative error
+is measured against a field that is small throughout and gets a looser bound.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+MACH, RE = 0.1, 1600.0
+MU = MACH / RE
+
+
+def per_field(a, b, n):
+    return [float((a[i * n:(i + 1) * n] - b[i * n:(i + 1) * n]).abs().max() /
+                  b[i * n:(i + 1) * n].abs().max()) for i in range(5)]
+
+
+def make(dims, precision, **kw):
+    import compact_schemes_b200 as cs
+    return cs.Solver(cs.tgv_config(None, dims=dims, precision=precision, **kw))
+
+
+@pytest.mark.parametrize("refine", [1, 0])
+def test_mixed_rhs_vs_oracle(cuda, refine):
+    """Mixed RHS against the FP64 oracle, relative to the size of the summed terms."""
+    import torch
+    dims = (48, 40, 32)
+    q = O.tgv_init(dims, MACH, 1e-4, 0)
+    ref, scale = O.rhs(q, MU, O.uniform_metrics(*dims), dims, [[1] * 3, [1] * 3], with_scale=True)
+    s = make(dims, 1, refine=refine)
+    out = torch.zeros(q.size, dtype=torch.float64, device="cuda")
+    s.rhs(torch.from_numpy(q).cuda(), out)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(5, -1)
+    err = max(np.abs(got[i] - ref.reshape(5, -1)[i]).max() / scale[i] for i in range(5))
+    assert err < 2e-6, err
+
+
+def test_mixed_100_steps_within_1e6(cuda):
+    import torch
+    import compact_schemes_b200 as cs
+    dims = (64, 64, 64)
+    n = 64 ** 3
+    q0 = torch.empty(5 * n, dtype=torch.float64, device="cuda")
+    cs.tgv_init(q0, dims, MACH, 1e-4, 0)
+    qp, qm = q0.clone(), q0.clone()
+    sp, sm = make(dims, 0), make(dims, 1)
+    for _ in range(100):
+        sp.step(qp, 0.0)
+        sm.step(qm, 0.0)
+    torch.cuda.synchronize()
+    errs = per_field(qm, qp, n)
+    print("mixed vs FP64 after 100 steps at 64^3, per field:", errs)
+    assert max(errs[:3] + errs[4:]) <= 1e-6, errs
+    assert errs[3] <= 1e-5, errs
+
+
+def test_config2_mixed_512_gcbc(cuda):
+    """512^3 mixed form with non-reflective GCBC on the x faces, periodic y/z,
+    100 RK steps; per-field error against the FP64 path (itself checked against
+    the CPU oracle at <= 256^3)."""
+    import torch
+    import compact_schemes_b200 as cs
+    dims = (512, 512, 512)
+    n = 512 ** 3
+    nbc = [[cs.BC_NON_REFLECTIVE, cs.BC_PERIODIC, cs.BC_PERIODIC]] * 2
+    q0 = torch.empty(5 * n, dtype=torch.float64, device="cuda")
+    cs.tgv_init(q0, dims, MACH, 1e-4, 0)
+    qp = q0.clone()
+    sp = make(dims, 0, nbc=nbc, gcbc=True)
+    for _ in range(100):
+        sp.step(qp, 0.0)
+    sp.close()
+    qm = q0
+    sm = make(dims, 1, nbc=nbc, gcbc=True)
+    for _ in range(100):
+        sm.step(qm, 0.0)
+    torch.cuda.synchronize()
+    errs = per_field(qm, qp, n)
+    print("512^3 GCBC mixed vs FP64 after 100 steps, per field:", errs)
+    assert all(np.isfinite(errs))
+    assert max(errs[:3] + errs[4:]) <= 1e-6, errs
+    assert errs[3] <= 1e-4, errs
