@@ -139,6 +139,8 @@ struct cs_solver {
     double *dt_dev = nullptr;
     int64_t F[3] = {0, 0, 0};
     int tile[2][3] = {{8, 8, 8}, {8, 8, 16}};  // lines per tile: [gradient|flux][axis]
+    int pl[2][3] = {{0, 0, 0}, {0, 0, 0}};     // pipelined kernels per [gradient|flux][axis]
+    int nsm = 0;
     // optional per-pass event timing (eager path only)
     bool profiling = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof;
@@ -202,6 +204,8 @@ static PassArgs pass_args(cs_solver *s, int a, int kind) {
     p.nstart = s->ndf[0][a];
     p.nend = s->ndf[1][a];
     p.tl = s->tile[kind][a];
+    p.pl = s->pl[kind][a];
+    p.nsm = s->nsm;
     p.viscous = s->cfg.viscous;
     p.tab = s->tab[a];
     p.cf = s->cf;
@@ -395,6 +399,10 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         delete s;
         return set_error(CS_ERR_INVALID, "precision %d", cfg->precision);
     }
+    if (cfg->schedule < CS_SCHED_AUTO || cfg->schedule > CS_SCHED_PIPELINE) {
+        delete s;
+        return set_error(CS_ERR_INVALID, "schedule %d", cfg->schedule);
+    }
     int smem_max = 0, dev = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
@@ -422,13 +430,23 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
                 }
                 s->tile[k][a] = 8;
             }
-            if (bytes(s->tile[k][a]) > (size_t)smem_max) {
+            // producer/consumer form: two staging buffers of pl_tile_for() lines
+            const bool pl_fits = 2 * bytes(pl_tile_for(s->tab[a]->lt, elem == 4)) <= (size_t)smem_max;
+            if (cfg->schedule == CS_SCHED_PIPELINE && !pl_fits) {
+                delete s;
+                return set_error(CS_ERR_UNSUPPORTED, "axis %d: the pipelined %s passes need %zu bytes of shared "
+                                 "memory", a, elem == 8 ? "FP64" : "mixed",
+                                 2 * bytes(pl_tile_for(s->tab[a]->lt, elem == 4)));
+            }
+            s->pl[k][a] = cfg->schedule == CS_SCHED_PIPELINE && pl_fits;
+            if (!s->pl[k][a] && bytes(s->tile[k][a]) > (size_t)smem_max) {
                 delete s;
                 return set_error(CS_ERR_UNSUPPORTED,
                                  "axis %d: lines of %d points do not fit the fused %s passes (%zu bytes of shared "
                                  "memory per 8-line tile)", a, llen(s->d, a), elem == 8 ? "FP64" : "mixed", bytes(8));
             }
         }
+    if (cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) s->nsm = 1;
     compute_interface_coeffs(s->cf);
     const double hx = cfg->dx, hy = cfg->dy, hz = cfg->dz;
     std::memset(&s->ph, 0, sizeof s->ph);

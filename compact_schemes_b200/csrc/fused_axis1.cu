@@ -6,6 +6,7 @@ namespace csb {
 
 template <>
 int launch_grad<1>(const PassArgs &a, const double *q, bool dtred, cudaStream_t st) {
+    if (a.pl) return launch_grad_pl<1>(a, q, dtred, st);
     if (a.tl == 16) return launch_grad_tl<1, 16>(a, q, dtred, st);
     return launch_grad_tl<1, 8>(a, q, dtred, st);
 }
@@ -13,6 +14,7 @@ int launch_grad<1>(const PassArgs &a, const double *q, bool dtred, cudaStream_t 
 template <>
 int launch_flux<1>(const PassArgs &a, int mode, const double *q, const double *qn, double *qout,
                    double *drva, const RkParams &rk, cudaStream_t st) {
+    if (a.pl) return launch_flux_pl<1>(a, mode, q, qn, qout, drva, rk, st);
     if (a.tl == 16) return launch_flux_tl<1, 16>(a, mode, q, qn, qout, drva, rk, st);
     return launch_flux_tl<1, 8>(a, mode, q, qn, qout, drva, rk, st);
 }

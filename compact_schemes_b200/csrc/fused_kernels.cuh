@@ -310,7 +310,9 @@ struct PassArgs {
     int lxi, let;
     int64_t F;
     int nstart, nend;
-    int tl;        // lines per tile (8 or 16)
+    int tl;        // lines per tile (8 or 16) of the one-phase kernels
+    int pl;        // nonzero: run the producer/consumer (pipelined) kernels
+    int nsm;       // multiprocessors of the device (persistent grid)
     int viscous;
     const DeviceTables *tab;
     Coeffs cf;
@@ -319,6 +321,15 @@ struct PassArgs {
     double *rhs;   // [5][lmx]
     unsigned long long *dtacc;
 };
+
+// Tile width of the pipelined passes for chunk length LT and element type T:
+// 8 lines for lines of up to 256 (FP64) / 512 (FP32) points, else 4, so that
+// two staging buffers fit in shared memory side by side.
+template <int LT, typename T>
+constexpr int pl_tile() {
+    return (sizeof(T) == 8 ? LT <= 8 : LT <= 16) ? 8 : 4;
+}
+inline int pl_tile_for(int lt, bool fp32) { return (fp32 ? lt <= 16 : lt <= 8) ? 8 : 4; }
 
 template <typename KernelT>
 inline int set_smem(KernelT kern, size_t bytes) {
@@ -390,7 +401,13 @@ int launch_flux_tl(const PassArgs &a, int mode, const double *q, const double *q
     }
 }
 
-// Per-axis entry points (fused_axis{0,1,2}.cu).
+// Per-axis entry points (fused_axis{0,1,2}.cu); they run the pipelined
+// kernels (pipeline_axis{0,1,2}.cu) when PassArgs::pl is set.
+template <int AXIS>
+int launch_grad_pl(const PassArgs &a, const double *q, bool dtred, cudaStream_t st);
+template <int AXIS>
+int launch_flux_pl(const PassArgs &a, int mode, const double *q, const double *qn, double *qout,
+                   double *drva, const RkParams &rk, cudaStream_t st);
 template <int AXIS>
 int launch_grad(const PassArgs &a, const double *q, bool dtred, cudaStream_t st);
 template <int AXIS>

@@ -41,48 +41,53 @@ __device__ __forceinline__ void deriv_row(int j, int n, int nstart, int nend, do
     else if (j == n - 2) { a = nend ? kAlpha : kAlpha10; c = a; }
 }
 
-// FP32 solve of the derivative of NF fields (FP32 lines in shared memory)
-// with FP64 right-hand sides and, if refine, one FP64-residual refinement.
+// FP32 solve of the derivative of one FP32 line in shared memory with FP64
+// right-hand sides and, if refine, one FP64-residual refinement; the result
+// overwrites the line.
+template <int LT>
+__device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTables<float> &tab, int nstart,
+                                              int nend, const Coeffs &cf, int refine) {
+    const int n = tab.n;
+    const int len = lane_len(lane, LT, tab.p, tab.last_len);
+    double r64[LT];
+    deriv_rhs<LT, double, float>(line, n, lane, nstart, nend, nullptr, cf, r64);
+    float x[1][LT];
+#pragma unroll
+    for (int t = 0; t < LT; ++t) x[0][t] = (float)r64[t];
+    warp_solve<LT, 1, float>(tab, x, lane);
+    if (refine) {
+        const float xm0 = __shfl_up_sync(0xffffffffu, x[0][LT - 1], 1);
+        const float xp0 = __shfl_down_sync(0xffffffffu, x[0][0], 1);
+        float e[1][LT];
+#pragma unroll
+        for (int t = 0; t < LT; ++t) {
+            const int j = lane * LT + t;
+            double a, cc;
+            deriv_row(j, n, nstart, nend, a, cc);
+            const double xm = t > 0 ? (double)x[0][t > 0 ? t - 1 : 0] : (double)xm0;
+            double xp = (double)xp0;
+#pragma unroll
+            for (int u = 0; u + 1 < LT; ++u)
+                if (u == t && t + 1 < len) xp = (double)x[0][u + 1];
+            const double res = r64[t] - (a * xm + (double)x[0][t] + cc * xp);
+            e[0][t] = j < n ? (float)res : 0.0f;
+        }
+        warp_solve<LT, 1, float>(tab, e, lane);
+#pragma unroll
+        for (int t = 0; t < LT; ++t) x[0][t] += e[0][t];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < LT; ++t)
+        if (lane * LT + t < n) line[LineLayout<LT>::pos_ct(lane, t)] = x[0][t];
+}
+
+// solve_line_mx for the NF fields of this warp's line of the tile.
 template <int LT, int TL, int NF>
 __device__ __forceinline__ void solve_fields_mx(float *sm, int w, int lane, const DevTables<float> &tab,
                                                 int nstart, int nend, const Coeffs &cf, int refine) {
-    const int n = tab.n;
-    const int len = lane_len(lane, LT, tab.p, tab.last_len);
 #pragma unroll 1
-    for (int c = 0; c < NF; ++c) {
-        float *line = field_line32<LT, TL>(sm, c, w);
-        double r64[LT];
-        deriv_rhs<LT, double, float>(line, n, lane, nstart, nend, nullptr, cf, r64);
-        float x[1][LT];
-#pragma unroll
-        for (int t = 0; t < LT; ++t) x[0][t] = (float)r64[t];
-        warp_solve<LT, 1, float>(tab, x, lane);
-        if (refine) {
-            const float xm0 = __shfl_up_sync(0xffffffffu, x[0][LT - 1], 1);
-            const float xp0 = __shfl_down_sync(0xffffffffu, x[0][0], 1);
-            float e[1][LT];
-#pragma unroll
-            for (int t = 0; t < LT; ++t) {
-                const int j = lane * LT + t;
-                double a, cc;
-                deriv_row(j, n, nstart, nend, a, cc);
-                const double xm = t > 0 ? (double)x[0][t > 0 ? t - 1 : 0] : (double)xm0;
-                double xp = (double)xp0;
-#pragma unroll
-                for (int u = 0; u + 1 < LT; ++u)
-                    if (u == t && t + 1 < len) xp = (double)x[0][u + 1];
-                const double res = r64[t] - (a * xm + (double)x[0][t] + cc * xp);
-                e[0][t] = j < n ? (float)res : 0.0f;
-            }
-            warp_solve<LT, 1, float>(tab, e, lane);
-#pragma unroll
-            for (int t = 0; t < LT; ++t) x[0][t] += e[0][t];
-        }
-        __syncwarp();
-#pragma unroll
-        for (int t = 0; t < LT; ++t)
-            if (lane * LT + t < n) line[LineLayout<LT>::pos_ct(lane, t)] = x[0][t];
-    }
+    for (int c = 0; c < NF; ++c) solve_line_mx<LT>(field_line32<LT, TL>(sm, c, w), lane, tab, nstart, nend, cf, refine);
 }
 
 // FP32 shadow values of one point from the FP64 state (thermo in FP64).
@@ -380,7 +385,13 @@ int launch_flux_mx_tl(const MixedArgs &a, int mode, const double *qn, double *qo
     }
 }
 
-// Per-axis entry points (fused_mixed_axis{0,1,2}.cu).
+// Per-axis entry points (fused_mixed_axis{0,1,2}.cu); they run the pipelined
+// kernels (pipeline_mixed_axis{0,1,2}.cu) when PassArgs::pl is set.
+template <int AXIS>
+int launch_grad_mx_pl(const MixedArgs &m, const double *q, bool first, cudaStream_t st);
+template <int AXIS>
+int launch_flux_mx_pl(const MixedArgs &m, int mode, const double *qn, double *qout, bool shadow_out,
+                      double *drva, const RkParams &rk, cudaStream_t st);
 template <int AXIS>
 int launch_grad_mx(const MixedArgs &a, const double *q, bool first, cudaStream_t st);
 template <int AXIS>

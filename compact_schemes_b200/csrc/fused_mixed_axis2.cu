@@ -6,6 +6,7 @@ namespace csb {
 
 template <>
 int launch_grad_mx<2>(const MixedArgs &a, const double *q, bool first, cudaStream_t st) {
+    if (a.base.pl) return launch_grad_mx_pl<2>(a, q, first, st);
     if (a.base.tl == 16) return launch_grad_mx_tl<2, 16>(a, q, first, st);
     return launch_grad_mx_tl<2, 8>(a, q, first, st);
 }
@@ -13,6 +14,7 @@ int launch_grad_mx<2>(const MixedArgs &a, const double *q, bool first, cudaStrea
 template <>
 int launch_flux_mx<2>(const MixedArgs &a, int mode, const double *qn, double *qout, bool shadow_out,
                       double *drva, const RkParams &rk, cudaStream_t st) {
+    if (a.base.pl) return launch_flux_mx_pl<2>(a, mode, qn, qout, shadow_out, drva, rk, st);
     if (a.base.tl == 16) return launch_flux_mx_tl<2, 16>(a, mode, qn, qout, shadow_out, drva, rk, st);
     return launch_flux_mx_tl<2, 8>(a, mode, qn, qout, shadow_out, drva, rk, st);
 }

@@ -122,3 +122,75 @@ __device__ __forceinline__ void tile_sync() {
 }
 
 }  // namespace csb
+
+namespace csb {
+
+// Role-relative traversal for the two-role (pipelined) passes: NT threads of one
+// role (rtid = 0..NT-1) cover a tile of TL lines.  x: TPL = max(32, NT / TL)
+// consecutive threads per line (warp w handles lines w, w + NT/32, ... when
+// TPL is 32); y/z: thread t covers line t % TL, rows t / TL + (NT / TL) k.
+template <int AXIS, int TL, int NT, int UNROLL = 1, typename Fn>
+__device__ __forceinline__ void tile_for_each_r(int rtid, int64_t line0, int64_t F, int n, int lxi, int let,
+                                                Fn &&fn) {
+    if (AXIS == 0) {
+        constexpr int TPL = NT / TL >= 32 ? NT / TL : 32;
+        for (int l = rtid / TPL; l < TL; l += NT / TPL) {
+            const int64_t fidx = line0 + l;
+            if (fidx >= F) break;
+            const int64_t base = fidx * n;
+#pragma unroll UNROLL
+            for (int j = rtid % TPL; j < n; j += TPL) fn(l, j, base + j);
+        }
+    } else {
+        const int l = rtid % TL;
+        const int64_t fidx = line0 + l;
+        if (fidx < F) {
+            const int64_t base = line_base<AXIS>(fidx, lxi, let), s = line_stride<AXIS>(lxi, let);
+#pragma unroll UNROLL
+            for (int j = rtid / TL; j < n; j += NT / TL) fn(l, j, base + j * s);
+        }
+    }
+}
+
+// Chunked read-modify-write form of tile_for_each_r (see tile_for_each_chunked).
+template <int AXIS, int TL, int NT, int P, typename FnLoad, typename FnStore>
+__device__ __forceinline__ void tile_for_each_r_chunked(int rtid, int64_t line0, int64_t F, int n, int lxi,
+                                                        int let, FnLoad &&load, FnStore &&store) {
+    constexpr int TPL = AXIS == 0 ? (NT / TL >= 32 ? NT / TL : 32) : NT / TL;
+    const int lfirst = AXIS == 0 ? rtid / TPL : rtid % TL;
+    const int lstep = AXIS == 0 ? NT / TPL : TL;
+    const int j0 = AXIS == 0 ? rtid % TPL : rtid / TL;
+    const int64_t s = line_stride<AXIS>(lxi, let);
+    for (int l = lfirst; l < TL; l += lstep) {
+        const int64_t fidx = line0 + l;
+        if (fidx >= F) break;
+        const int64_t base = line_base<AXIS>(fidx, lxi, let);
+        for (int jc = j0; jc < n; jc += P * TPL) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const int j = jc + p * TPL;
+                if (j < n) load(p, l, j, base + j * s);
+            }
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const int j = jc + p * TPL;
+                if (j < n) store(p, l, j, base + j * s);
+            }
+        }
+    }
+}
+
+// Named CTA barriers for the two-role (pipelined) passes (barrier 0 is
+// __syncthreads).  bar.sync waits until `count` threads have arrived;
+// bar.arrive counts the caller without waiting.
+__device__ __forceinline__ void named_bar_sync(int id, int count) {
+    __syncwarp();
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_bar_arrive(int id, int count) {
+    __syncwarp();
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+constexpr int kBarFull0 = 1;  // + buffer: tile staged, ready to solve
+
+}  // namespace csb

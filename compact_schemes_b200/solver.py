@@ -19,15 +19,18 @@ class SolverConfig(ctypes.Structure):
                 ("umf", ctypes.c_double * 3), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
                 ("dz", ctypes.c_double), ("cfl", ctypes.c_double), ("gcbc", ctypes.c_int),
                 ("use_graph", ctypes.c_int), ("tile", ctypes.c_int * 3 * 2),
-                ("precision", ctypes.c_int), ("refine", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("refine", ctypes.c_int), ("schedule", ctypes.c_int)]
 
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+SCHED_AUTO = 0
+SCHED_ONEPHASE = 1
+SCHED_PIPELINE = 2
 
 
 def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, dims=None,
-               nbc=None, gcbc=False, tile=None, precision=PREC_FP64, refine=1):
+               nbc=None, gcbc=False, tile=None, precision=PREC_FP64, refine=1, schedule=SCHED_AUTO):
     """Taylor-Green box [0,2pi)^3 in CANARD units: mu = rho0 U0 L / Re with U0 = Mach."""
     lxi, let, lze = dims if dims is not None else (n, n, n)
     c = SolverConfig()
@@ -46,6 +49,7 @@ def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, di
     c.use_graph = int(use_graph)
     c.precision = int(precision)
     c.refine = int(refine)
+    c.schedule = int(schedule)
     if tile is not None:
         for k in range(2):
             for a in range(3):

@@ -210,6 +210,11 @@ typedef struct cs_solver cs_solver;
                            FP64-residual refinement sweep), FP64 state, RK accumulation
                            and thermodynamics */
 
+#define CS_SCHED_AUTO 0     /* the measured-faster schedule: one-phase on B200 */
+#define CS_SCHED_ONEPHASE 1 /* each CTA loads a tile, solves it, stores it (tile[][] applies) */
+#define CS_SCHED_PIPELINE 2 /* persistent CTAs: memory warps store tile k-1 and stage tile k+1
+                               while solver warps solve tile k; error where the tiles do not fit */
+
 typedef struct {
     int lxi, let, lze;  /* points per axis */
     int nbc[2][3];      /* boundary code per face / axis (both faces of an axis periodic or both physical) */
@@ -226,6 +231,7 @@ typedef struct {
                            form uses 8 for y */
     int precision;      /* CS_PREC_FP64 or CS_PREC_MIXED */
     int refine;         /* mixed: one FP64-residual refinement sweep per line solve (1) or none (0) */
+    int schedule;       /* CS_SCHED_*: how a pass overlaps its line solves with its HBM traffic */
 } cs_solver_config;
 
 int cs_solver_create(cs_solver **out, const cs_solver_config *cfg);

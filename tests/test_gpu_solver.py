@@ -143,6 +143,31 @@ def test_graph_step_equals_eager(cuda):
     assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("dims,gcbc", [((64, 64, 64), False), ((96, 64, 80), False), ((64, 48, 32), True)])
+def test_pipelined_schedule_bit_identical(cuda, dims, gcbc, precision):
+    """The two-role (pipelined) passes do the one-phase passes' arithmetic in
+    the same order: RHS and three RK steps agree bit for bit."""
+    import torch
+    import compact_schemes_b200 as cs
+    from compact_schemes_b200.solver import SCHED_ONEPHASE, SCHED_PIPELINE
+    nbc = [[cs.BC_NON_REFLECTIVE, cs.BC_PERIODIC, cs.BC_PERIODIC]] * 2 if gcbc else None
+    q0 = O.tgv_init(dims, MACH, 1e-4, 5)
+    outs = []
+    for sched in (SCHED_ONEPHASE, SCHED_PIPELINE):
+        s = solver(dims, use_graph=False, schedule=sched, precision=precision, nbc=nbc, gcbc=gcbc)
+        q = dev(q0)
+        r = torch.empty_like(q)
+        s.rhs(q, r)
+        for _ in range(3):
+            s.step(q, 0.0)
+        torch.cuda.synchronize()
+        outs.append((r.view(torch.int64).clone(), q.view(torch.int64).clone()))
+        s.close()
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][1], outs[1][1])
+
+
 def test_100_steps_within_1e10(cuda):
     import torch
     dims = (32, 32, 32)
