@@ -53,6 +53,22 @@ def declare(L):
     L.cs_solver_last_dt.argtypes = [vp, ctypes.POINTER(f64)]
     L.cs_solver_dt_device.argtypes = [vp, pp]
     L.cs_tgv_init.argtypes = [vp, i32, i32, i32, f64, f64, ctypes.c_uint64, vp]
+    from .ensemble import EnsembleTuning
+    pt = ctypes.POINTER(EnsembleTuning)
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    L.cs_ensemble_create.argtypes = [pp, i32, ctypes.POINTER(SolverConfig)]
+    L.cs_ensemble_destroy.argtypes = [vp]
+    L.cs_ensemble_state_size.argtypes = [vp, i64p]
+    L.cs_ensemble_box_offset.argtypes = [vp, i32, i64p]
+    L.cs_ensemble_step.argtypes = [vp, vp, vp]
+    L.cs_ensemble_last_dt.argtypes = [vp, ctypes.POINTER(f64)]
+    L.cs_ensemble_set_tuning.argtypes = [vp, pt]
+    L.cs_ensemble_get_tuning.argtypes = [vp, pt]
+    L.cs_ensemble_autotune.argtypes = [vp, vp, i32, pt, ctypes.POINTER(f64), vp]
+    for name in ("cs_ensemble_create", "cs_ensemble_destroy", "cs_ensemble_state_size", "cs_ensemble_box_offset",
+                 "cs_ensemble_step", "cs_ensemble_last_dt", "cs_ensemble_set_tuning", "cs_ensemble_get_tuning",
+                 "cs_ensemble_autotune"):
+        getattr(L, name).restype = i32
     L.cs_solver_profile_begin.argtypes = [vp]
     L.cs_solver_profile_end.argtypes = [vp, vp, vp]
     for name in ("cs_solver_create", "cs_solver_destroy", "cs_solver_rhs", "cs_solver_stage",

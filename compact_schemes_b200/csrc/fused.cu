@@ -190,6 +190,25 @@ struct PassTimer {
     }
 };
 
+int bc_ndf(int code) {
+    if (code == CS_BC_NON_REFLECTIVE || code == CS_BC_WALL_INVISCID || code == CS_BC_WALL_VISCOUS ||
+        code == CS_BC_INTER_CURV) return 0;
+    if (code == CS_BC_INTER_STRAIGHT || code == CS_BC_INTER_SUBDOMAINS || code == CS_BC_PERIODIC) return 1;
+    return -1;
+}
+
+void uniform_phys(const cs_solver_config &cfg, Phys &ph) {
+    const double hx = cfg.dx, hy = cfg.dy, hz = cfg.dz;
+    std::memset(&ph, 0, sizeof ph);
+    ph.M[0][0] = hy * hz;
+    ph.M[1][1] = hx * hz;
+    ph.M[2][2] = hx * hy;
+    ph.J = 1.0 / (hx * hy * hz);
+    ph.mu = cfg.mu;
+    for (int c = 0; c < 3; ++c) ph.umf[c] = cfg.umf[c];
+    ph.rr1 = ph.M[0][0] * ph.M[0][0] + ph.M[1][1] * ph.M[1][1] + ph.M[2][2] * ph.M[2][2];
+}
+
 static int64_t fsize(const cs_dcomp &d, int a) {
     return a == 0 ? (int64_t)d.let * d.lze : (a == 1 ? (int64_t)d.lxi * d.lze : (int64_t)d.lxi * d.let);
 }
@@ -375,12 +394,8 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
     s->d = cs_dcomp{cfg->lxi * cfg->let * cfg->lze, cfg->lxi, cfg->let, cfg->lze};
     for (int f = 0; f < 2; ++f)
         for (int a = 0; a < 3; ++a) {
-            const int b = cfg->nbc[f][a];
-            if (b == CS_BC_NON_REFLECTIVE || b == CS_BC_WALL_INVISCID || b == CS_BC_WALL_VISCOUS ||
-                b == CS_BC_INTER_CURV) s->ndf[f][a] = 0;
-            else if (b == CS_BC_INTER_STRAIGHT || b == CS_BC_INTER_SUBDOMAINS || b == CS_BC_PERIODIC)
-                s->ndf[f][a] = 1;
-            else { delete s; return set_error(CS_ERR_INVALID, "boundary code %d", b); }
+            s->ndf[f][a] = bc_ndf(cfg->nbc[f][a]);
+            if (s->ndf[f][a] < 0) { delete s; return set_error(CS_ERR_INVALID, "boundary code %d", cfg->nbc[f][a]); }
         }
     for (int a = 0; a < 3; ++a) {
         const int n = llen(s->d, a);
@@ -448,15 +463,7 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         }
     if (cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) s->nsm = 1;
     compute_interface_coeffs(s->cf);
-    const double hx = cfg->dx, hy = cfg->dy, hz = cfg->dz;
-    std::memset(&s->ph, 0, sizeof s->ph);
-    s->ph.M[0][0] = hy * hz;
-    s->ph.M[1][1] = hx * hz;
-    s->ph.M[2][2] = hx * hy;
-    s->ph.J = 1.0 / (hx * hy * hz);
-    s->ph.mu = cfg->mu;
-    for (int c = 0; c < 3; ++c) s->ph.umf[c] = cfg->umf[c];
-    s->ph.rr1 = s->ph.M[0][0] * s->ph.M[0][0] + s->ph.M[1][1] * s->ph.M[1][1] + s->ph.M[2][2] * s->ph.M[2][2];
+    uniform_phys(*cfg, s->ph);
     const int64_t lmx = s->d.lmx;
     bool ok = cudaMalloc(&s->q1, 5 * lmx * sizeof(double)) == cudaSuccess &&
               cudaMalloc(&s->grad, 12 * lmx * sizeof(double)) == cudaSuccess &&

@@ -54,10 +54,13 @@ struct RkParams {
     double *dt_out;
 };
 
+// CG: the maxima were reduced earlier in the same launch by other CTAs, so
+// they are read from L2 (ld.global.cg) rather than through a possibly stale L1.
+template <bool CG = false>
 __device__ __forceinline__ double rk_dt(const RkParams &rk) {
     if (rk.dt_fixed > 0.0) return rk.dt_fixed;
-    const double m1 = __longlong_as_double((long long)rk.dtacc[0]);
-    const double m2 = __longlong_as_double((long long)rk.dtacc[1]);
+    const double m1 = __longlong_as_double((long long)(CG ? __ldcg(rk.dtacc) : rk.dtacc[0]));
+    const double m2 = __longlong_as_double((long long)(CG ? __ldcg(rk.dtacc + 1) : rk.dtacc[1]));
     const double a = rk.cfl / m1, b = 0.5 / m2;
     return a < b ? a : b;
 }
@@ -115,20 +118,16 @@ __device__ __forceinline__ void solve_fields(double *sm, int w, int lane, const 
     }
 }
 
-// ----------------------------------------------------------------------------
-// gradient pass: G[AXIS][c] = d/dxi_AXIS of (u, v, w, T)
-// ----------------------------------------------------------------------------
+// One tile of the gradient pass: lines line0 .. line0+TL-1 (TL * 32 threads;
+// sm holds 4 * TL line slots).
 template <int LT, int AXIS, int TL, bool DTRED>
-__global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_GRAD_MINB : 1)
-k_grad(const double *__restrict__ q, double *__restrict__ g, DevTables<double> tab, int lxi, int let,
-       int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf, Phys ph,
-       unsigned long long *__restrict__ dtacc) {
+__device__ __forceinline__ void grad_tile(double *sm, int64_t line0, const double *__restrict__ q,
+                                          double *__restrict__ g, const DevTables<double> &tab, int lxi, int let,
+                                          int64_t lmx, int64_t F, int nstart, int nend, const Coeffs &cf,
+                                          const Phys &ph, unsigned long long *__restrict__ dtacc) {
     using L = LineLayout<LT>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sm = reinterpret_cast<double *>(smem_raw);
     const int n = tab.n;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t line0 = (int64_t)blockIdx.x * TL;
     double m1 = 0.0, m2 = 0.0;
     tile_for_each<AXIS, TL, CSB_GRAD_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         const Prim s = primitives(__ldg(q + gi), __ldg(q + lmx + gi), __ldg(q + 2 * lmx + gi),
@@ -175,6 +174,19 @@ k_grad(const double *__restrict__ q, double *__restrict__ g, DevTables<double> t
 }
 
 // ----------------------------------------------------------------------------
+// gradient pass: G[AXIS][c] = d/dxi_AXIS of (u, v, w, T)
+// ----------------------------------------------------------------------------
+template <int LT, int AXIS, int TL, bool DTRED>
+__global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_GRAD_MINB : 1)
+k_grad(const double *__restrict__ q, double *__restrict__ g, DevTables<double> tab, int lxi, int let,
+       int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf, Phys ph,
+       unsigned long long *__restrict__ dtacc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    grad_tile<LT, AXIS, TL, DTRED>(reinterpret_cast<double *>(smem_raw), (int64_t)blockIdx.x * TL, q, g, tab, lxi,
+                                   let, lmx, F, nstart, nend, cf, ph, dtacc);
+}
+
+// ----------------------------------------------------------------------------
 // flux pass
 // ----------------------------------------------------------------------------
 enum FluxMode { kWrite = 0, kAccum = 1, kAccumRk = 2, kWriteRk = 3 };
@@ -182,7 +194,9 @@ enum FluxMode { kWrite = 0, kAccum = 1, kAccumRk = 2, kWriteRk = 3 };
 // Flux components F[m][AXIS] at one point from the state and the gradients
 // (calc_fluxes_pre_compute_kernel<Visc>, src/cuda/kernels/physics.hpp:42-193,
 // with tau / heat flux of calc_viscous_shear_stress_final_kernel, :285-333).
-template <int AXIS, bool VISC>
+// CG: the gradients were written earlier in the same launch by other CTAs
+// (ensemble launch) and are read from L2 (ld.global.cg).
+template <int AXIS, bool VISC, bool CG = false>
 __device__ __forceinline__ void point_flux(const double *__restrict__ q, const double *__restrict__ g,
                                            int64_t lmx, int64_t gi, const Phys &ph, double (&fl)[5]) {
     const double q0 = __ldg(q + gi), q1 = __ldg(q + lmx + gi), q2 = __ldg(q + 2 * lmx + gi);
@@ -190,7 +204,7 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
     double gr[12];
     if (VISC) {
 #pragma unroll
-        for (int k = 0; k < 12; ++k) gr[k] = __ldg(g + k * lmx + gi);
+        for (int k = 0; k < 12; ++k) gr[k] = CG ? __ldcg(g + k * lmx + gi) : __ldg(g + k * lmx + gi);
     }
     const Prim s = primitives(q0, q1, q2, q3, q4);
     const double *Ma = ph.M[AXIS];
@@ -228,21 +242,22 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
     }
 }
 
-template <int LT, int AXIS, int TL, int MODE, bool VISC>
-__global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_FLUX_MINB : 1)
-k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__restrict__ rhs,
-       const double *__restrict__ qn, double *__restrict__ qout, double *__restrict__ drva,
-       DevTables<double> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend,
-       Coeffs cf, Phys ph, RkParams rk) {
+// One tile of the flux pass (TL * 32 threads; sm holds 5 * TL line slots).
+// CG: the RHS accumulator, gradients and CFL maxima come from other CTAs of
+// the same launch (ensemble) and are read from L2.
+template <int LT, int AXIS, int TL, int MODE, bool VISC, bool CG = false>
+__device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const double *__restrict__ q,
+                                          const double *__restrict__ g, double *__restrict__ rhs,
+                                          const double *__restrict__ qn, double *__restrict__ qout,
+                                          double *__restrict__ drva, const DevTables<double> &tab, int lxi, int let,
+                                          int64_t lmx, int64_t F, int nstart, int nend, const Coeffs &cf,
+                                          const Phys &ph, const RkParams &rk) {
     using L = LineLayout<LT>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sm = reinterpret_cast<double *>(smem_raw);
     const int n = tab.n;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t line0 = (int64_t)blockIdx.x * TL;
     tile_for_each<AXIS, TL, CSB_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         double fl[5];
-        point_flux<AXIS, VISC>(q, g, lmx, gi, ph, fl);
+        point_flux<AXIS, VISC, CG>(q, g, lmx, gi, ph, fl);
         const int pj = L::pos(j);
 #pragma unroll
         for (int m = 0; m < 5; ++m) field_line<LT, TL>(sm, m, l)[pj] = fl[m];
@@ -264,9 +279,9 @@ k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__res
     tile_sync<AXIS, TL>();
     double dtk = 0.0;
     if (MODE >= kAccumRk) {
-        const double dt = rk_dt(rk);
+        const double dt = rk_dt<CG>(rk);
         dtk = xmul(dt / rk.div, ph.J);
-        if (rk.dt_out && blockIdx.x == 0 && threadIdx.x == 0) *rk.dt_out = dt;
+        if (rk.dt_out && line0 == 0 && threadIdx.x == 0) *rk.dt_out = dt;
     }
     if (MODE == kWrite) {
         tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
@@ -283,7 +298,7 @@ k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__res
             [&](int p, int l, int j, int64_t gi) {
 #pragma unroll
                 for (int m = 0; m < 5; ++m) {
-                    rv[p][m] = MODE == kWriteRk ? 0.0 : rhs[m * lmx + gi];
+                    rv[p][m] = MODE == kWriteRk ? 0.0 : (CG ? __ldcg(rhs + m * lmx + gi) : rhs[m * lmx + gi]);
                     if (MODE >= kAccumRk) qv[p][m] = qn[m * lmx + gi];
                 }
             },
@@ -303,6 +318,22 @@ k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__res
     }
 }
 
+template <int LT, int AXIS, int TL, int MODE, bool VISC>
+__global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_FLUX_MINB : 1)
+k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__restrict__ rhs,
+       const double *__restrict__ qn, double *__restrict__ qout, double *__restrict__ drva,
+       DevTables<double> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend,
+       Coeffs cf, Phys ph, RkParams rk) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    flux_tile<LT, AXIS, TL, MODE, VISC>(reinterpret_cast<double *>(smem_raw), (int64_t)blockIdx.x * TL, q, g, rhs, qn,
+                                        qout, drva, tab, lxi, let, lmx, F, nstart, nend, cf, ph, rk);
+}
+
+
+// Derivative closure of a boundary code: 0 physical, 1 interface / periodic, -1 unknown.
+int bc_ndf(int code);
+// Metrics, Jacobian and viscosity of the uniform grid of a solver configuration.
+void uniform_phys(const cs_solver_config &cfg, Phys &ph);
 
 // Everything one pass needs, independent of the solver object.
 struct PassArgs {

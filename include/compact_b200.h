@@ -35,6 +35,7 @@ extern "C" {
 #define CS_ERR_UNSUPPORTED (-3) /* line too long/short for the kernels */
 #define CS_ERR_ALLOC (-4)       /* device allocation failed */
 #define CS_ERR_STATE (-5)       /* call order (e.g. deriv before deriv_setup) */
+#define CS_ERR_TIMEOUT (-6)     /* a bounded device-side wait ran out; that call's results are invalid */
 
 /* Boundary codes, src/common/parameters.hpp:46-52. */
 #define CS_BC_NON_REFLECTIVE 10
@@ -266,6 +267,49 @@ int cs_solver_profile_end(cs_solver *s, double ms[CS_PASS_KINDS], int launches[C
  * (no reference implementation: physics::init is empty, src/physics_pc.hpp:78-81). */
 int cs_tgv_init(double *q, int lxi, int let, int lze, double mach, double noise_amp,
                 uint64_t seed, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Batched ensemble: independent boxes of uneven sizes advanced together.
+ * No reference counterpart (the reference advances one block per rank,
+ * driver/canard.cu:132-224); each box is a cs_solver_config (FP64, uniform
+ * grid, no GCBC; every axis 8..256 points).  One persistent launch per RK
+ * stage pulls tiles of lines of all boxes from a device work queue ordered so
+ * that each box's gradient, x-, y- and z-flux phases follow the phase they
+ * depend on; a step (4 stages) replays one captured CUDA graph.  Per box the
+ * arithmetic is that of cs_solver_step with a CFL time step, so every box's
+ * result is bit-identical to stepping it with its own cs_solver.
+ * The state of all boxes is one packed device array: box b's q [5][lmx_b]
+ * starts at cs_ensemble_box_offset(b).
+ * ------------------------------------------------------------------------- */
+typedef struct cs_ensemble cs_ensemble;
+
+typedef struct {
+    int window;      /* queue lag: phase p of the box of size rank r is queued at slot r + p * window
+                        (0 = number of boxes: every box's gradients first, then x fluxes, ...) */
+    int tile;        /* lines per work item: 4 or 8 */
+    int ctas_per_sm; /* resident CTAs per SM of the persistent grid; 0 = as many as fit */
+    int chunk;       /* tiles per work item taken from the queue: 1..64 */
+} cs_ensemble_tuning;
+
+int cs_ensemble_create(cs_ensemble **out, int nbox, const cs_solver_config *boxes);
+int cs_ensemble_destroy(cs_ensemble *e);
+/* Length in doubles of the packed state, and the offset of box b in it. */
+int cs_ensemble_state_size(const cs_ensemble *e, int64_t *n_doubles);
+int cs_ensemble_box_offset(const cs_ensemble *e, int box, int64_t *offset);
+/* One RK step of every box, in place on the packed device state q; dt per box
+ * from the CFL formula of calc_time_step on that box.  No host sync. */
+int cs_ensemble_step(cs_ensemble *e, double *q, void *stream);
+/* dt of every box in the last step (synchronizes); CS_ERR_TIMEOUT if a
+ * dependency wait of the work queue ran out since the previous check. */
+int cs_ensemble_last_dt(cs_ensemble *e, double *dt_host);
+int cs_ensemble_set_tuning(cs_ensemble *e, const cs_ensemble_tuning *t);
+int cs_ensemble_get_tuning(const cs_ensemble *e, cs_ensemble_tuning *t);
+/* Autotuner: times `reps` steps of every candidate tuning (tile width x tiles
+ * per work item x queue lag) on a scratch copy of q (q is not modified),
+ * keeps the fastest and returns it with its milliseconds per step.
+ * Synchronizes. */
+int cs_ensemble_autotune(cs_ensemble *e, const double *q, int reps, cs_ensemble_tuning *best, double *best_ms,
+                         void *stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,128 @@
+"""Batched ensemble on the GPU: every box bit-identical to its own per-box
+solver (which the solver tests pin to the FP64 oracle), for every tuning,
+plus one box against the oracle directly."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+BOXES = [((32, 48, 40), 0.1, 1600.0), ((64, 32, 32), 0.25, 500.0), ((48, 48, 48), 0.05, 3000.0),
+         ((96, 32, 40), 0.2, 800.0), ((40, 128, 24), 0.15, 1200.0)]
+
+
+def _state(ens, boxes, seed0=0):
+    import torch
+    import compact_schemes_b200 as cs
+    q = torch.zeros(ens.state_size(), dtype=torch.float64, device="cuda:0")
+    for b, (dims, mach, _) in enumerate(boxes):
+        cs.tgv_init(ens.box_view(q, b), dims, mach, 1e-4, seed0 + b)
+    return q
+
+
+def _per_box(boxes, q0, ens, steps, viscous=True, nbc=None):
+    import torch
+    import compact_schemes_b200 as cs
+    outs, dts = [], []
+    for b, (dims, mach, re) in enumerate(boxes):
+        s = cs.Solver(cs.tgv_config(None, mach=mach, re=re, dims=dims, viscous=viscous, nbc=nbc))
+        qb = ens.box_view(q0, b).clone()
+        for _ in range(steps):
+            s.step(qb)
+        torch.cuda.synchronize()
+        outs.append(qb)
+        dts.append(s.last_dt())
+        s.close()
+    return outs, dts
+
+
+@pytest.mark.parametrize("viscous", [True, False])
+def test_ensemble_matches_per_box_solvers(cuda, viscous):
+    import torch
+    import compact_schemes_b200 as cs
+    cfgs = cs.ensemble_tgv(BOXES, viscous=viscous)
+    ens = cs.Ensemble(cfgs)
+    q = _state(ens, BOXES)
+    ref, dts = _per_box(BOXES, q, ens, 3, viscous=viscous)
+    for _ in range(3):
+        ens.step(q)
+    edt = ens.last_dt()
+    for b in range(len(BOXES)):
+        assert torch.equal(ens.box_view(q, b), ref[b]), b
+        assert edt[b] == dts[b]
+    ens.close()
+
+
+@pytest.mark.parametrize("tuning", [dict(window=0, tile=8, chunk=1), dict(window=2, tile=8, chunk=16),
+                                    dict(window=1, tile=4, chunk=3), dict(window=3, tile=4, ctas_per_sm=1)])
+def test_ensemble_tunings_bit_identical(cuda, tuning):
+    import torch
+    import compact_schemes_b200 as cs
+    ens = cs.Ensemble(cs.ensemble_tgv(BOXES))
+    q = _state(ens, BOXES, 7)
+    ref, _ = _per_box(BOXES, q, ens, 2)
+    ens.set_tuning(**tuning)
+    for _ in range(2):
+        ens.step(q)
+    ens.last_dt()
+    for b in range(len(BOXES)):
+        assert torch.equal(ens.box_view(q, b), ref[b]), b
+    ens.close()
+
+
+def test_ensemble_physical_closures(cuda):
+    import torch
+    import compact_schemes_b200 as cs
+    nbc = [[cs.BC_NON_REFLECTIVE] * 3] * 2
+    boxes = BOXES[:3]
+    cfgs = [cs.tgv_config(None, mach=m, re=r, dims=d, nbc=nbc) for d, m, r in boxes]
+    ens = cs.Ensemble(cfgs)
+    q = _state(ens, boxes, 3)
+    ref, _ = _per_box(boxes, q, ens, 2, nbc=nbc)
+    for _ in range(2):
+        ens.step(q)
+    ens.last_dt()
+    for b in range(len(boxes)):
+        assert torch.equal(ens.box_view(q, b), ref[b]), b
+
+
+def test_ensemble_box_against_oracle(cuda):
+    import compact_schemes_b200 as cs
+    ens = cs.Ensemble(cs.ensemble_tgv(BOXES))
+    q = _state(ens, BOXES, 11)
+    b = 3
+    dims, mach, re = BOXES[b]
+    qo = ens.box_view(q, b).cpu().numpy().copy()
+    ens.step(q)
+    ens.last_dt()
+    O.rk_step(qo, mach / re, O.uniform_metrics(*dims), dims, [[45] * 3, [45] * 3], cfl=0.5)
+    got = ens.box_view(q, b).cpu().numpy().reshape(5, -1)
+    ref = qo.reshape(5, -1)
+    err = max(np.abs(got[i] - ref[i]).max() / np.abs(ref[i]).max() for i in range(5))
+    assert err < 1e-12
+
+
+def test_ensemble_autotune_keeps_state(cuda):
+    import torch
+    import compact_schemes_b200 as cs
+    ens = cs.Ensemble(cs.ensemble_tgv(BOXES))
+    q = _state(ens, BOXES)
+    q0 = q.clone()
+    best, ms = ens.autotune(q, reps=2)
+    torch.cuda.synchronize()
+    assert torch.equal(q, q0)
+    assert ms > 0 and best["tile"] in (4, 8) and ens.tuning() == best
+    ref, _ = _per_box(BOXES, q, ens, 1)
+    ens.step(q)
+    ens.last_dt()
+    for b in range(len(BOXES)):
+        assert torch.equal(ens.box_view(q, b), ref[b]), b
+
+
+def test_ensemble_rejects_unsupported(cuda):
+    import compact_schemes_b200 as cs
+    with pytest.raises(cs.CSError, match="8..256"):
+        cs.Ensemble(cs.ensemble_tgv([((4, 32, 32), 0.1, 1000.0)]))
+    with pytest.raises(cs.CSError, match="FP64"):
+        cs.Ensemble([cs.tgv_config(None, dims=(32, 32, 32), precision=1)])
