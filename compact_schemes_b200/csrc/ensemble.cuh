@@ -84,9 +84,8 @@ __device__ __noinline__ void ens_item(const EnsArgs &a, int b, int64_t line0, do
     const double *qin = (stage == 0 ? a.q : a.q1) + bx.qoff;
     double *g = a.grad + bx.goff;
     constexpr int AX = KIND % 3;
-    // private copies: the compiler can keep them across the stores of the tile
-    const Phys ph = bx.ph;
-    const DevTables<double> tab = bx.tab[AX];
+    const Phys &ph = bx.ph;
+    const DevTables<double> &tab = bx.tab[AX];
     if (KIND < 3) {
         if (KIND == 0 && stage == 0)
             grad_tile<LT, 0, TL, true>(sm, line0, qin, g, tab, bx.lxi, bx.let, bx.lmx, bx.F[0], bx.nstart[0],
