@@ -69,6 +69,28 @@ def declare(L):
                  "cs_ensemble_step", "cs_ensemble_last_dt", "cs_ensemble_set_tuning", "cs_ensemble_get_tuning",
                  "cs_ensemble_autotune"):
         getattr(L, name).restype = i32
+    dp = ctypes.POINTER(f64)
+    L.cs_adjoint_create.argtypes = [pp, ctypes.POINTER(SolverConfig)]
+    L.cs_adjoint_destroy.argtypes = [vp]
+    L.cs_adjoint_deriv.argtypes = [vp, i32, i32, vp, vp, i32, i32, vp]
+    L.cs_rhs_jvp.argtypes = [vp, vp, vp, vp, vp]
+    L.cs_rhs_vjp.argtypes = [vp, vp, vp, vp, vp]
+    L.cs_adjoint_stages.argtypes = [vp, vp, f64, pp, vp, vp]
+    L.cs_step_jvp.argtypes = [vp, pp, f64, vp, vp, vp]
+    L.cs_step_vjp.argtypes = [vp, pp, f64, vp, vp, vp]
+    L.cs_kinetic_energy.argtypes = [vp, vp, dp, vp, vp]
+    L.cs_adjoint_gradient.argtypes = [vp, vp, i32, dp, i32, vp, dp, vp]
+    L.cs_point_flux.argtypes = [i32, i32, dp, dp, dp, f64, f64, dp, dp]
+    L.cs_point_flux_jvp.argtypes = [i32, i32, dp, dp, dp, dp, dp, f64, f64, dp, dp]
+    L.cs_point_flux_vjp.argtypes = [i32, i32, dp, dp, dp, dp, f64, f64, dp, dp, dp]
+    L.cs_point_prim.argtypes = [dp, dp]
+    L.cs_point_prim_jvp.argtypes = [dp, dp, dp]
+    L.cs_point_prim_vjp.argtypes = [dp, dp, dp]
+    for name in ("cs_adjoint_create", "cs_adjoint_destroy", "cs_adjoint_deriv", "cs_rhs_jvp", "cs_rhs_vjp",
+                 "cs_adjoint_stages", "cs_step_jvp", "cs_step_vjp", "cs_kinetic_energy", "cs_adjoint_gradient",
+                 "cs_point_flux", "cs_point_flux_jvp", "cs_point_flux_vjp", "cs_point_prim", "cs_point_prim_jvp",
+                 "cs_point_prim_vjp"):
+        getattr(L, name).restype = i32
     L.cs_solver_profile_begin.argtypes = [vp]
     L.cs_solver_profile_end.argtypes = [vp, vp, vp]
     for name in ("cs_solver_create", "cs_solver_destroy", "cs_solver_rhs", "cs_solver_stage",

@@ -1,0 +1,219 @@
+// adjoint.cuh -- device kernels of the tangent and adjoint RHS.
+//
+// The compact derivative along a line is D = A^-1 B (A tridiagonal, B the
+// explicit stencil with its closure rows: deriv_rhs).  Tangents apply D;
+// adjoints apply D^T = B^T A^-T: a solve with the transposed tridiagonal
+// matrix (its own precomputed tables, scheme kDerivT) followed by the
+// transposed stencil, whose closure columns are gathered from the four
+// boundary rows (physical rows, or the interface rows with their pbci / pbco
+// weights, numerics_device_pc.hpp:176-293).
+#pragma once
+
+#include "adjoint_point.cuh"
+#include "fused_kernels.cuh"
+
+namespace csb {
+
+// Column j of the closure rows 0, 1, n-2, n-1 of B.
+__device__ __forceinline__ double brow0(int j, int n, int nstart, const Coeffs &cf) {
+    if (nstart) return (j < kLmd ? cf.pbci[j] : 0.0) + (n - 1 - j < kLmd ? cf.pbco[n - 1 - j] : 0.0);
+    return j == 0 ? kAb00 : (j == 1 ? kAb01 : (j == 2 ? kAb02 : 0.0));
+}
+__device__ __forceinline__ double brow1(int j, int n, int nstart, const Coeffs &cf) {
+    if (nstart)
+        return (j < kLmd ? cf.pbci[kLmd + j] : 0.0) + (n - 1 - j < kLmd ? cf.pbco[kLmd + n - 1 - j] : 0.0);
+    return j == 0 ? -kAb10 : (j == 2 ? kAb10 : 0.0);
+}
+__device__ __forceinline__ double browm1(int j, int n, int nend, const Coeffs &cf) {
+    if (nend) return -((n - 1 - j < kLmd ? cf.pbci[n - 1 - j] : 0.0) + (j < kLmd ? cf.pbco[j] : 0.0));
+    return j == n - 1 ? -kAb00 : (j == n - 2 ? -kAb01 : (j == n - 3 ? -kAb02 : 0.0));
+}
+__device__ __forceinline__ double browm2(int j, int n, int nend, const Coeffs &cf) {
+    if (nend)
+        return -((n - 1 - j < kLmd ? cf.pbci[kLmd + n - 1 - j] : 0.0) + (j < kLmd ? cf.pbco[kLmd + j] : 0.0));
+    return j == n - 3 ? -kAb10 : (j == n - 1 ? kAb10 : 0.0);
+}
+
+// o = B^T z for this lane's rows (z: a line in shared memory).
+template <int LT>
+__device__ __forceinline__ void stencil_t(const double *z, int n, int lane, int nstart, int nend, const Coeffs &cf,
+                                          double (&o)[LT]) {
+    using L = LineLayout<LT>;
+    const double z0 = z[L::pos(0)], z1 = z[L::pos(1)], zm2 = z[L::pos(n - 2)], zm1 = z[L::pos(n - 1)];
+#pragma unroll
+    for (int t = 0; t < LT; ++t) {
+        const int j = lane * LT + t;
+        double s = 0.0;
+        if (j < n) {
+            // interior rows i in [2, n-3]: B[i][i+-1] = +-a, B[i][i+-2] = +-b
+            if (j - 1 >= 2 && j - 1 <= n - 3) s += kAa * z[L::pos(j - 1)];
+            if (j + 1 >= 2 && j + 1 <= n - 3) s -= kAa * z[L::pos(j + 1)];
+            if (j - 2 >= 2 && j - 2 <= n - 3) s += kBb * z[L::pos(j - 2)];
+            if (j + 2 >= 2 && j + 2 <= n - 3) s -= kBb * z[L::pos(j + 2)];
+            if (j < kLmd || j >= n - kLmd)
+                s += z0 * brow0(j, n, nstart, cf) + z1 * brow1(j, n, nstart, cf) + zm2 * browm2(j, n, nend, cf) +
+                     zm1 * browm1(j, n, nend, cf);
+        }
+        o[t] = s;
+    }
+}
+
+// out[f] (=|+=) scale * D (or D^T) in[f] along AXIS, field f = blockIdx.y;
+// one warp per line, 8 lines per CTA.
+template <int LT, int AXIS, bool TRANS>
+__global__ void __launch_bounds__(256) k_lines(const double *__restrict__ in, int64_t in_fs,
+                                               double *__restrict__ out, int64_t out_fs, int accum, double scale,
+                                               DevTables<double> tab, int lxi, int let, int64_t F, int nstart,
+                                               int nend, Coeffs cf) {
+    constexpr int TL = 8;
+    using L = LineLayout<LT>;
+    __shared__ double sm[TL * L::kSlot];
+    const int n = tab.n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t line0 = (int64_t)blockIdx.x * TL;
+    const double *src = in + blockIdx.y * in_fs;
+    double *dst = out + blockIdx.y * out_fs;
+    tile_for_each<AXIS, TL>(line0, F, n, lxi, let,
+                            [&](int l, int j, int64_t gi) { sm[l * L::kSlot + L::pos(j)] = src[gi]; });
+    tile_sync<AXIS, TL>();
+    if (line0 + w < F) {
+        double *line = sm + w * L::kSlot;
+        double d[1][LT];
+        if (!TRANS) {
+            deriv_rhs<LT, double, double>(line, n, lane, nstart, nend, nullptr, cf, d[0]);
+            warp_solve<LT, 1, double>(tab, d, lane);
+        } else {
+#pragma unroll
+            for (int t = 0; t < LT; ++t) d[0][t] = lane * LT + t < n ? line[L::pos_ct(lane, t)] : 0.0;
+            warp_solve<LT, 1, double>(tab, d, lane);
+            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < LT; ++t)
+                if (lane * LT + t < n) line[L::pos_ct(lane, t)] = d[0][t];
+            __syncwarp();
+            stencil_t<LT>(line, n, lane, nstart, nend, cf, d[0]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < LT; ++t)
+            if (lane * LT + t < n) line[L::pos_ct(lane, t)] = d[0][t];
+    }
+    tile_sync<AXIS, TL>();
+    tile_for_each<AXIS, TL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+        const double v = scale * sm[l * L::kSlot + L::pos(j)];
+        dst[gi] = accum ? dst[gi] + v : v;
+    });
+}
+
+// --------------------------------------------------------------- pointwise
+struct AdjPoint {
+    PointPhys ph;
+    int64_t lmx;
+    int viscous;
+};
+
+#define CSB_GRID_STRIDE(i, n) for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); \
+                                   i += (int64_t)gridDim.x * blockDim.x)
+
+// dphi = (dphi/dq) dq
+__global__ void k_prim_tan(const double *__restrict__ q, const double *__restrict__ dq, double *__restrict__ dphi,
+                           int64_t lmx) {
+    CSB_GRID_STRIDE(i, lmx) {
+        double qq[5], d[5], o[4];
+        for (int m = 0; m < 5; ++m) { qq[m] = q[m * lmx + i]; d[m] = dq[m * lmx + i]; }
+        prim_tan(qq, d, o);
+        for (int c = 0; c < 4; ++c) dphi[c * lmx + i] = o[c];
+    }
+}
+
+// dF[a][m] = (dF_a/dq) dq + (dF_a/dG) dG for every active axis a
+template <bool VISC>
+__global__ void k_flux_tan(const double *__restrict__ q, const double *__restrict__ G, const double *__restrict__ dq,
+                           const double *__restrict__ dG, double *__restrict__ dF, AdjPoint ap, int amask) {
+    const int64_t lmx = ap.lmx;
+    CSB_GRID_STRIDE(i, lmx) {
+        double qq[5], d[5], g[12], dg[12], o[5];
+        for (int m = 0; m < 5; ++m) { qq[m] = q[m * lmx + i]; d[m] = dq[m * lmx + i]; }
+        for (int k = 0; k < 12; ++k) {
+            g[k] = VISC ? G[k * lmx + i] : 0.0;
+            dg[k] = VISC ? dG[k * lmx + i] : 0.0;
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (!(amask >> a & 1)) continue;
+            flux_tan<VISC>(a, qq, g, d, dg, ap.ph, o);
+            for (int m = 0; m < 5; ++m) dF[(a * 5 + m) * lmx + i] = o[m];
+        }
+    }
+}
+
+// qbar = sum_a (dF_a/dq)^T mu_a,  Gbar = sum_a (dF_a/dG)^T mu_a
+template <bool VISC>
+__global__ void k_flux_adj(const double *__restrict__ q, const double *__restrict__ G, const double *__restrict__ mu,
+                           double *__restrict__ qbar, double *__restrict__ Gbar, AdjPoint ap, int amask) {
+    const int64_t lmx = ap.lmx;
+    CSB_GRID_STRIDE(i, lmx) {
+        double qq[5], g[12], qb[5] = {0, 0, 0, 0, 0}, gb[12], fb[5];
+        for (int m = 0; m < 5; ++m) qq[m] = q[m * lmx + i];
+        for (int k = 0; k < 12; ++k) {
+            g[k] = VISC ? G[k * lmx + i] : 0.0;
+            gb[k] = 0.0;
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (!(amask >> a & 1)) continue;
+            for (int m = 0; m < 5; ++m) fb[m] = mu[(a * 5 + m) * lmx + i];
+            flux_adj<VISC>(a, qq, g, fb, ap.ph, qb, gb);
+        }
+        for (int m = 0; m < 5; ++m) qbar[m * lmx + i] = qb[m];
+        if (VISC)
+            for (int k = 0; k < 12; ++k) Gbar[k * lmx + i] = gb[k];
+    }
+}
+
+// out = scale * (qbar + (dphi/dq)^T phibar)
+__global__ void k_prim_adj(const double *__restrict__ q, const double *__restrict__ qbar,
+                           const double *__restrict__ phibar, double *__restrict__ out, double scale, int64_t lmx,
+                           int have_phibar) {
+    CSB_GRID_STRIDE(i, lmx) {
+        double qq[5], qb[5], pb[4];
+        for (int m = 0; m < 5; ++m) { qq[m] = q[m * lmx + i]; qb[m] = qbar[m * lmx + i]; }
+        if (have_phibar) {
+            for (int c = 0; c < 4; ++c) pb[c] = phibar[c * lmx + i];
+            prim_adj(qq, pb, qb);
+        }
+        for (int m = 0; m < 5; ++m) out[m * lmx + i] = scale * qb[m];
+    }
+}
+
+// y = a * x + b * y  (n values)
+__global__ void k_axpby(double a, const double *__restrict__ x, double b, double *__restrict__ y, int64_t n) {
+    CSB_GRID_STRIDE(i, n) y[i] = a * x[i] + b * y[i];
+}
+
+// Kinetic energy 0.5 * sum (m.m)/rho * dV (block partial sums) and its
+// gradient with respect to q.
+__global__ void k_kinetic(const double *__restrict__ q, int64_t lmx, double dv, double *__restrict__ partial,
+                          double *__restrict__ seed) {
+    __shared__ double red[256];
+    double acc = 0.0;
+    CSB_GRID_STRIDE(i, lmx) {
+        const double r = q[i], m1 = q[lmx + i], m2 = q[2 * lmx + i], m3 = q[3 * lmx + i];
+        const double mm = m1 * m1 + m2 * m2 + m3 * m3, ri = 1.0 / r;
+        acc += 0.5 * mm * ri * dv;
+        if (seed) {
+            seed[i] = -0.5 * mm * ri * ri * dv;
+            seed[lmx + i] = m1 * ri * dv;
+            seed[2 * lmx + i] = m2 * ri * dv;
+            seed[3 * lmx + i] = m3 * ri * dv;
+            seed[4 * lmx + i] = 0.0;
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+}  // namespace csb

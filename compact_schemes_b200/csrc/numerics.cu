@@ -74,6 +74,13 @@ static bool host_tables_for(int n, int scheme, int nstart, int nend, double af, 
     bool cyclic = false;
     if (scheme == kDeriv) {
         deriv_rows(n, nstart, nend, a.data(), b.data(), c.data());
+    } else if (scheme == kDerivT) {
+        std::vector<double> a0(n), c0(n);
+        deriv_rows(n, nstart, nend, a0.data(), b.data(), c0.data());
+        for (int i = 0; i < n; ++i) {
+            a[i] = i > 0 ? c0[i - 1] : 0.0;
+            c[i] = i < n - 1 ? a0[i + 1] : 0.0;
+        }
     } else {
         cyclic = nstart && nend;
         filter_rows(n, cyclic, af, a.data(), b.data(), c.data());

@@ -311,6 +311,56 @@ int cs_ensemble_get_tuning(const cs_ensemble *e, cs_ensemble_tuning *t);
 int cs_ensemble_autotune(cs_ensemble *e, const double *q, int reps, cs_ensemble_tuning *best, double *best_ms,
                          void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Tangent-linear and adjoint of the RHS and of the RK step (no reference
+ * counterpart).  For a cs_solver_config (FP64, no GCBC, lines of at most
+ * 512 points), with dt held fixed:
+ *   R'(q) dq    = sum_a D_a [dF_a/dq dq + dF_a/dG dG],   dG_b = D_b (dphi/dq dq)
+ *   R'(q)^T l   = dF/dq^T mu + dphi/dq^T sum_b D_b^T (dF/dG^T mu)_b,   mu_a = D_a^T l
+ * where D_a = A^-1 B is the compact derivative along axis a (its transpose is
+ * a solve with A^T followed by B^T), F_a the flux of calc_fluxes_pre_compute
+ * (src/cuda/kernels/physics.hpp:42-193) and phi = (u, v, w, T).
+ * All arrays are device [nf][lmx] fields unless named _host.
+ * ------------------------------------------------------------------------- */
+typedef struct cs_adjoint cs_adjoint;
+
+int cs_adjoint_create(cs_adjoint **out, const cs_solver_config *cfg);
+int cs_adjoint_destroy(cs_adjoint *a);
+/* out[f] (= or +=) D_axis in[f] (transpose = 0) or D_axis^T in[f], f < nfields. */
+int cs_adjoint_deriv(cs_adjoint *a, int axis, int transpose, const double *in, double *out, int nfields,
+                     int accumulate, void *stream);
+int cs_rhs_jvp(cs_adjoint *a, const double *q, const double *dq, double *dR, void *stream);
+int cs_rhs_vjp(cs_adjoint *a, const double *q, const double *lam, double *out, void *stream);
+/* Stage states of one step with time step dt: stages[0] = q^n (copied unless
+ * stages[0] == qn), stages[k] = q^(k-1) for k = 1..3; q_next = q^(n+1) (may be null). */
+int cs_adjoint_stages(cs_adjoint *a, const double *qn, double dt, double *const stages[4], double *q_next,
+                      void *stream);
+/* Tangent / adjoint of one RK step about the stage states of cs_adjoint_stages. */
+int cs_step_jvp(cs_adjoint *a, const double *const stages[4], double dt, const double *dq_n, double *dq_next,
+                void *stream);
+int cs_step_vjp(cs_adjoint *a, const double *const stages[4], double dt, const double *lam_next, double *lam_n,
+                void *stream);
+/* J = 1/2 sum (m.m)/rho dx dy dz (synchronizes when J_host is set) and dJ/dq (may be null). */
+int cs_kinetic_energy(cs_adjoint *a, const double *q, double *J_host, double *dJdq, void *stream);
+/* dJ/dq0 of J = kinetic energy after nsteps steps with time steps dt_host[s]:
+ * forward sweep keeping a checkpoint every `every` steps, then a reverse sweep
+ * that recomputes each segment's stage states from its checkpoint and applies
+ * cs_step_vjp step by step.  Synchronizes. */
+int cs_adjoint_gradient(cs_adjoint *a, const double *q0, int nsteps, const double *dt_host, int every,
+                        double *grad_q0, double *J_host, void *stream);
+/* Host-side pointwise linearizations (no device memory): the flux F_axis(q, G)
+ * with G[b*4 + c] = d(phi_c)/d(xi_b), metrics M (row-major 3x3), Jacobian J,
+ * viscosity mu, frame velocity umf; and the primitives phi(q). */
+int cs_point_flux(int axis, int viscous, const double q[5], const double G[12], const double M[9], double J,
+                  double mu, const double umf[3], double F[5]);
+int cs_point_flux_jvp(int axis, int viscous, const double q[5], const double G[12], const double dq[5],
+                      const double dG[12], const double M[9], double J, double mu, const double umf[3], double dF[5]);
+int cs_point_flux_vjp(int axis, int viscous, const double q[5], const double G[12], const double Fbar[5],
+                      const double M[9], double J, double mu, const double umf[3], double qbar[5], double Gbar[12]);
+int cs_point_prim(const double q[5], double phi[4]);
+int cs_point_prim_jvp(const double q[5], const double dq[5], double dphi[4]);
+int cs_point_prim_vjp(const double q[5], const double phibar[4], double qbar[5]);
+
 #ifdef __cplusplus
 }
 #endif
