@@ -52,7 +52,168 @@ def parse():
     p.add_argument("--n", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-mixed", action="store_true")
+    p.add_argument("--no-ensemble", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
+
+
+def ensemble_section(args):
+    """64 seeded Taylor-Green boxes, each axis in {32,48,64,96,128}, Mach in
+    [0.05,0.3), Re in [400,3200), FP64: the autotuned ensemble step against
+    looping one graph-replayed Solver per box, both on device-resident state."""
+    import torch
+    import compact_schemes_b200 as cs
+    boxes = cs.draw_boxes(64, 0)
+    npts = cs.ensemble.ensemble_points(boxes)
+    cfgs = cs.ensemble_tgv(boxes)
+    ens = cs.Ensemble(cfgs)
+    q = torch.zeros(ens.state_size(), dtype=torch.float64, device="cuda")
+    for b, (d, m, _) in enumerate(boxes):
+        cs.tgv_init(ens.box_view(q, b), d, m, 1e-4, b)
+    tuning, tune_ms = ens.autotune(q, reps=2)
+    steps = 5
+    for _ in range(2):
+        ens.step(q)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        ens.step(q)
+    e1.record()
+    torch.cuda.synchronize()
+    ens.last_dt()  # raises on a dependency-wait timeout
+    t_ens = e0.elapsed_time(e1) / steps
+    solvers = [cs.Solver(c) for c in cfgs]
+    views = [ens.box_view(q, b) for b in range(len(boxes))]
+    for sv, v in zip(solvers, views):
+        sv.step(v)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        for sv, v in zip(solvers, views):
+            sv.step(v)
+    e1.record()
+    torch.cuda.synchronize()
+    t_loop = e0.elapsed_time(e1) / steps
+    for sv in solvers:
+        sv.close()
+    ens.close()
+    rate = lambda ms: npts * 4 / (ms * 1e-3) / 1e6
+    return {"workload": "64 seeded TGV boxes, axes in {32,48,64,96,128}, FP64", "points": npts,
+            "value": rate(t_ens), "unit": UNIT, "ms_per_step": t_ens,
+            "loop_per_box_value": rate(t_loop), "loop_ms_per_step": t_loop,
+            "speedup_vs_loop": t_loop / t_ens, "tuning": tuning, "autotune_ms_per_step": tune_ms,
+            "launches_per_step": 4, "steps": steps}
+
+
+def adjoint_section(args):
+    """Gradient of the kinetic energy after 50 steps of the 128^3 Taylor-Green
+    box with respect to the initial density (velocity, pressure fixed),
+    checkpoint every 10 steps, time steps frozen at the CFL trajectory's."""
+    import torch
+    import compact_schemes_b200 as cs
+    n, nsteps, every = 128, 50, 10
+    lmx = n ** 3
+    cfg = cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=False)
+    s = cs.Solver(cfg)
+    free0 = torch.cuda.mem_get_info()[0]
+    a = cs.Adjoint(cfg)
+    free1 = torch.cuda.mem_get_info()[0]
+    q0 = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
+    cs.tgv_init(q0, (n, n, n), MACH, 1e-4, 0)
+    qr, dts = q0.clone(), []
+    for _ in range(nsteps):
+        s.step(qr, 0.0)
+        dts.append(s.last_dt())
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    e0, e1 = ev(), ev()
+    qf = q0.clone()
+    e0.record()
+    for dt in dts:
+        s.step(qf, dt)
+    e1.record()
+    torch.cuda.synchronize()
+    t_fwd = e0.elapsed_time(e1)
+    lam = torch.empty_like(q0)
+    a.gradient(q0, dts, every, lam)
+    e0.record()
+    J = a.gradient(q0, dts, every, lam)
+    e1.record()
+    torch.cuda.synchronize()
+    t_grad = e0.elapsed_time(e1)
+    # one reverse step: stage recomputation + step adjoint, against one forward step
+    st = [torch.empty_like(q0) for _ in range(4)]
+    out = torch.empty_like(q0)
+    e0.record()
+    for _ in range(5):
+        a.stages(q0, dts[0], st)
+        a.step_vjp(st, dts[0], lam, out)
+    e1.record()
+    torch.cuda.synchronize()
+    t_rev_step = e0.elapsed_time(e1) / 5
+    sweep_bytes = a.gradient_bytes(nsteps, every)
+    # d J / d rho0 and central differences along 8 seeded Gaussian directions
+    lv = lam.view(5, -1)
+    u = q0.view(5, -1)[1:4] / q0.view(5, -1)[0]
+    g = lv[0] + (lv[1:4] * u).sum(0) + 0.5 * lv[4] * (u * u).sum(0)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    eps, fd_err = 1e-6, []
+
+    def j_of(rho):
+        qq = q0.clone().view(5, -1)
+        p = 0.4 * (qq[4] - 0.5 * qq[0] * (u * u).sum(0))
+        qq[0] = rho
+        qq[1:4] = rho * u
+        qq[4] = p / 0.4 + 0.5 * rho * (u * u).sum(0)
+        qq = qq.reshape(-1)
+        for dt in dts:
+            s.step(qq, dt)
+        return a.kinetic_energy(qq)
+
+    rho0 = q0.view(5, -1)[0].clone()
+    for _ in range(8):
+        v = torch.randn(lmx, dtype=torch.float64, device="cuda", generator=gen)
+        fd = (j_of(rho0 + eps * v) - j_of(rho0 - eps * v)) / (2 * eps)
+        fd_err.append(abs(float((g * v).sum()) - fd) / abs(fd))
+    # forward/adjoint dot product for the 50-step map
+    x = torch.randn(5 * lmx, dtype=torch.float64, device="cuda", generator=gen)
+    y = torch.randn(5 * lmx, dtype=torch.float64, device="cuda", generator=gen)
+    q, dx = q0.clone(), x.clone()
+    for dt in dts:
+        a.stages(q, dt, st)
+        a.step_jvp(st, dt, dx, out)
+        dx, out = out, dx
+        s.step(q, dt)
+    lam_y = torch.empty_like(q0)
+    a_grad_dot = _adjoint_map(a, s, q0, dts, every, y, lam_y)
+    lhs, rhs = float((y * dx).sum()), float((lam_y * x).sum())
+    a.close()
+    s.close()
+    return {"workload": "128^3 TGV, 50 steps, checkpoint every 10, dJ/drho0 of J = kinetic energy", "J": J,
+            "forward_ms": t_fwd, "gradient_ms": t_grad, "gradient_over_forward": t_grad / t_fwd,
+            "reverse_step_ms": t_rev_step, "forward_step_ms": t_fwd / nsteps,
+            "adjoint_step_over_forward_step": t_rev_step / (t_fwd / nsteps),
+            "memory_bytes": {"adjoint_scratch": free0 - free1, "checkpoint_sweep": sweep_bytes,
+                             "peak": free0 - free1 + sweep_bytes},
+            "fd_rel_err_8_dirs": fd_err, "fd_eps": eps,
+            "dot_product_rel_err": abs(lhs - rhs) / abs(lhs), "dt": "frozen at the CFL trajectory's"}
+
+
+def _adjoint_map(a, s, q0, dts, every, y, lam_out):
+    """lam_out = A^T y for the tangent A of len(dts) steps (recomputing stages)."""
+    import torch
+    traj, q = [], q0.clone()
+    for dt in dts:
+        traj.append(q.clone())
+        s.step(q, dt)
+    st = [torch.empty_like(q0) for _ in range(4)]
+    lam, out = y.clone(), torch.empty_like(q0)
+    for k in reversed(range(len(dts))):
+        a.stages(traj[k], dts[k], st)
+        a.step_vjp(st, dts[k], lam, out)
+        lam, out = out, lam
+    lam_out.copy_(lam)
+    return True
 
 
 def peaks():
@@ -325,6 +486,16 @@ def run_ours(args):
                "sample": "1 RK stage of the %d^3 Taylor-Green box in %.1f s (FP64 oracle, "
                          "C++/OpenMP restatement of the reference kernels)" % (n, t)}
 
+    ensemble = adjoint = None
+    if rank == 0 and world == 1:
+        s.close()
+        if not args.no_ensemble:
+            ensemble = ensemble_section(args)
+            torch.cuda.empty_cache()
+        if not args.no_adjoint:
+            adjoint = adjoint_section(args)
+            torch.cuda.empty_cache()
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
@@ -337,6 +508,7 @@ def run_ours(args):
                            "l2": "inputs larger than L2 (state 671 MB + gradients 1.6 GB), no flush",
                            "parallelism": "replicas" if world > 1 else "single GPU"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed,
+                "ensemble": ensemble, "adjoint": adjoint,
                 "gpu_launches": 24 * args.steps, "clocks": clocks,
                 "passes": per_pass,
                 "stage_model": {"bytes_per_point": STAGE_BYTES, "ms_per_stage": stage_ms,

@@ -80,6 +80,8 @@ def declare(L):
     L.cs_step_vjp.argtypes = [vp, pp, f64, vp, vp, vp]
     L.cs_kinetic_energy.argtypes = [vp, vp, dp, vp, vp]
     L.cs_adjoint_gradient.argtypes = [vp, vp, i32, dp, i32, vp, dp, vp]
+    L.cs_adjoint_gradient_bytes.argtypes = [vp, i32, i32, ctypes.POINTER(sz)]
+    L.cs_adjoint_gradient_bytes.restype = i32
     L.cs_point_flux.argtypes = [i32, i32, dp, dp, dp, f64, f64, dp, dp]
     L.cs_point_flux_jvp.argtypes = [i32, i32, dp, dp, dp, dp, dp, f64, f64, dp, dp]
     L.cs_point_flux_vjp.argtypes = [i32, i32, dp, dp, dp, dp, f64, f64, dp, dp, dp]

@@ -64,6 +64,11 @@ class Adjoint:
                                       stream_ptr(stream)))
         return J.value
 
+    def gradient_bytes(self, nsteps, every):
+        b = ctypes.c_size_t()
+        check(lib().cs_adjoint_gradient_bytes(self._h, int(nsteps), int(every), ctypes.byref(b)))
+        return b.value
+
     def gradient(self, q0, dts, every, grad_out, stream=None):
         """dJ/dq0 of the kinetic energy after len(dts) steps; returns J."""
         n = len(dts)

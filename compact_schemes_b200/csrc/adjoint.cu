@@ -127,8 +127,9 @@ static int rhs_jvp(cs_adjoint *a, const double *q, const double *dq, double *dR,
     return CS_OK;
 }
 
-// out = scale * R'(q)^T lam
-static int rhs_vjp(cs_adjoint *a, const double *q, const double *lam, double *out, double scale, cudaStream_t st) {
+// w = scale * R'(q)^T lam; out = w (if set); acc_out = (acc_in or acc_out) + w (if set)
+static int rhs_vjp(cs_adjoint *a, const double *q, const double *lam, double *out, double scale, cudaStream_t st,
+                   const double *acc_in = nullptr, double *acc_out = nullptr) {
     const int64_t lmx = a->lmx;
     const bool visc = a->cfg.viscous != 0;
     if (visc)
@@ -147,18 +148,14 @@ static int rhs_vjp(cs_adjoint *a, const double *q, const double *lam, double *ou
             have_pb = true;
         }
     }
-    k_prim_adj<<<kPointBlocks, 256, 0, st>>>(q, a->qbar, a->phi4, out, scale, lmx, have_pb ? 1 : 0);
+    k_prim_adj<<<kPointBlocks, 256, 0, st>>>(q, a->qbar, a->phi4, out, scale, lmx, have_pb ? 1 : 0, acc_in,
+                                             acc_out);
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }
 
 static double stage_c(const cs_adjoint *a, int k, double dt) { return dt / (4 - k) * a->ph.J; }
 
-static int axpby(double x_a, const double *x, double y_b, double *y, int64_t n, cudaStream_t st) {
-    k_axpby<<<kPointBlocks, 256, 0, st>>>(x_a, x, y_b, y, n);
-    CSB_CUDA(cudaGetLastError());
-    return CS_OK;
-}
 
 }  // namespace csb
 
@@ -268,8 +265,8 @@ int cs_step_jvp(cs_adjoint *a, const double *const stages[4], double dt, const d
         double *nxt = k == 3 ? dq_next : (k % 2 == 0 ? a->t1 : a->t2);
         if (int rc = rhs_jvp(a, stages[k], cur, a->t3, st)) return rc;
         // nxt = dq_n - c_k dR
-        CSB_CUDA(cudaMemcpyAsync(nxt, dq_n, n5 * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        if (int rc = axpby(-stage_c(a, k, dt), a->t3, 1.0, nxt, n5, st)) return rc;
+        k_xpay<<<kPointBlocks, 256, 0, st>>>(dq_n, -stage_c(a, k, dt), a->t3, nxt, n5);
+        CSB_CUDA(cudaGetLastError());
         cur = nxt;
     }
     return CS_OK;
@@ -279,13 +276,12 @@ int cs_step_vjp(cs_adjoint *a, const double *const stages[4], double dt, const d
                 void *stream) {
     if (!a || !stages || !lam_next || !lam_n || lam_next == lam_n) return set_error(CS_ERR_INVALID, "bad argument");
     cudaStream_t st = (cudaStream_t)stream;
-    const int64_t n5 = 5 * a->lmx;
-    CSB_CUDA(cudaMemcpyAsync(lam_n, lam_next, n5 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    // lam_n = lam_next + w_3 + w_2 + w_1 + w_0, w_k = -c_k R'(q^(k-1))^T lam_k, lam_(k-1) = w_k
     const double *cur = lam_next;
     for (int k = 3; k >= 0; --k) {
-        double *w = k % 2 == 1 ? a->t1 : a->t2;
-        if (int rc = rhs_vjp(a, stages[k], cur, w, -stage_c(a, k, dt), st)) return rc;
-        if (int rc = axpby(1.0, w, 1.0, lam_n, n5, st)) return rc;
+        double *w = k == 0 ? nullptr : (k % 2 == 1 ? a->t1 : a->t2);
+        if (int rc = rhs_vjp(a, stages[k], cur, w, -stage_c(a, k, dt), st, k == 3 ? lam_next : nullptr, lam_n))
+            return rc;
         cur = w;
     }
     return CS_OK;
@@ -305,6 +301,13 @@ int cs_kinetic_energy(cs_adjoint *a, const double *q, double *J_host, double *dJ
         for (double v : part) s += v;
         *J_host = s;
     }
+    return CS_OK;
+}
+
+int cs_adjoint_gradient_bytes(const cs_adjoint *a, int nsteps, int every, size_t *bytes) {
+    if (!a || !bytes || nsteps < 1 || every < 1) return set_error(CS_ERR_INVALID, "bad argument");
+    const int nseg = (nsteps + every - 1) / every, segmax = every < nsteps ? every : nsteps;
+    *bytes = (size_t)(nseg + 1 + 4LL * segmax + 2) * 5 * a->lmx * sizeof(double);
     return CS_OK;
 }
 

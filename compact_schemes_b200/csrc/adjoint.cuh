@@ -169,10 +169,11 @@ __global__ void k_flux_adj(const double *__restrict__ q, const double *__restric
     }
 }
 
-// out = scale * (qbar + (dphi/dq)^T phibar)
+// w = scale * (qbar + (dphi/dq)^T phibar); out = w (if set); acc_out =
+// (acc_in if set, else acc_out) + w (if acc_out is set).
 __global__ void k_prim_adj(const double *__restrict__ q, const double *__restrict__ qbar,
                            const double *__restrict__ phibar, double *__restrict__ out, double scale, int64_t lmx,
-                           int have_phibar) {
+                           int have_phibar, const double *__restrict__ acc_in, double *__restrict__ acc_out) {
     CSB_GRID_STRIDE(i, lmx) {
         double qq[5], qb[5], pb[4];
         for (int m = 0; m < 5; ++m) { qq[m] = q[m * lmx + i]; qb[m] = qbar[m * lmx + i]; }
@@ -180,13 +181,18 @@ __global__ void k_prim_adj(const double *__restrict__ q, const double *__restric
             for (int c = 0; c < 4; ++c) pb[c] = phibar[c * lmx + i];
             prim_adj(qq, pb, qb);
         }
-        for (int m = 0; m < 5; ++m) out[m * lmx + i] = scale * qb[m];
+        for (int m = 0; m < 5; ++m) {
+            const double w = scale * qb[m];
+            if (out) out[m * lmx + i] = w;
+            if (acc_out) acc_out[m * lmx + i] = (acc_in ? acc_in[m * lmx + i] : acc_out[m * lmx + i]) + w;
+        }
     }
 }
 
-// y = a * x + b * y  (n values)
-__global__ void k_axpby(double a, const double *__restrict__ x, double b, double *__restrict__ y, int64_t n) {
-    CSB_GRID_STRIDE(i, n) y[i] = a * x[i] + b * y[i];
+// z = x + a * y  (n values)
+__global__ void k_xpay(const double *__restrict__ x, double a, const double *__restrict__ y, double *__restrict__ z,
+                       int64_t n) {
+    CSB_GRID_STRIDE(i, n) z[i] = x[i] + a * y[i];
 }
 
 // Kinetic energy 0.5 * sum (m.m)/rho * dV (block partial sums) and its

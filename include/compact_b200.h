@@ -348,6 +348,9 @@ int cs_kinetic_energy(cs_adjoint *a, const double *q, double *J_host, double *dJ
  * cs_step_vjp step by step.  Synchronizes. */
 int cs_adjoint_gradient(cs_adjoint *a, const double *q0, int nsteps, const double *dt_host, int every,
                         double *grad_q0, double *J_host, void *stream);
+/* Device bytes cs_adjoint_gradient allocates for its sweeps (checkpoints,
+ * running state, one segment's stage states, two adjoint states). */
+int cs_adjoint_gradient_bytes(const cs_adjoint *a, int nsteps, int every, size_t *bytes);
 /* Host-side pointwise linearizations (no device memory): the flux F_axis(q, G)
  * with G[b*4 + c] = d(phi_c)/d(xi_b), metrics M (row-major 3x3), Jacobian J,
  * viscosity mu, frame velocity umf; and the primitives phi(q). */
