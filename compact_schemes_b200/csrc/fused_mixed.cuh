@@ -3,10 +3,10 @@
 // FP64 master state q and FP64 RK accumulation; what the line solves consume
 // is FP32:
 //   * an FP32 "deviation shadow" of the stage state, (rho - rho0, u, v, w,
-//     p - p0) with the free-stream rho0 = 1, p0 = 1/gamma (CANARD units).  It
-//     is formed from q in FP64 (pressure and temperature recovered from total
-//     energy in FP64, where low-Mach cancellation needs it), so FP32 keeps its
-//     relative precision on the small deviations;
+//     T - T0) with the free-stream rho0 = 1, T0 = gamma p0 / rho0 = 1 (CANARD
+//     units).  It is formed from q in FP64 (pressure and temperature
+//     recovered from total energy in FP64, where low-Mach cancellation needs
+//     it), so FP32 keeps its relative precision on the small deviations;
 //   * FP32 gradients of (u, v, w, T - T0) and an FP32 RHS accumulator R;
 //   * fluxes evaluated in FP64 from the shadow and rounded once to FP32 when
 //     staged.  They use the pressure deviation: with constant metrics the
@@ -98,14 +98,12 @@ __device__ __forceinline__ void shadow_from_q(double q0, double q1, double q2, d
     sh[1] = (float)s.u;
     sh[2] = (float)s.v;
     sh[3] = (float)s.w;
-    sh[4] = (float)(s.p - kP0);
+    sh[4] = (float)(s.T - kT0);
 }
 
-// T - T0 from the shadow deviations, in FP64: with gamma p0 = T0 rho0,
-// T - T0 = (gamma dp - T0 drho) / (rho0 + drho), free of cancellation.
-__device__ __forceinline__ double temp_dev(float dr, float dp) {
-    return ((double)kGam * (double)dp - kT0 * (double)dr) / (kRho0 + (double)dr);
-}
+// p - p0 from the shadow deviations, in FP64: with p = rho T / gamma and
+// gamma p0 = rho0 T0 = 1, p - p0 = (drho + dT + drho dT) / gamma.
+__device__ __forceinline__ double pres_dev(double dr, double dT) { return (dr + dT + dr * dT) * (1.0 / kGam); }
 
 // ----------------------------------------------------------------------------
 // gradient pass (FIRST: reads the FP64 state, writes the shadow, reduces CFL)
@@ -134,7 +132,7 @@ k_grad_mx(const double *__restrict__ q, float *__restrict__ sh, float *__restric
             u = s5[1];
             v = s5[2];
             wv = s5[3];
-            tp = (float)temp_dev(s5[0], s5[4]);
+            tp = s5[4];
             const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
             double rr2 = 0.0;
 #pragma unroll
@@ -144,11 +142,11 @@ k_grad_mx(const double *__restrict__ q, float *__restrict__ sh, float *__restric
             m1 = fmax(m1, xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi));
             m2 = fmax(m2, s.ri * ph.mu * ph.rr1 * ssi * ssi);
         } else {
-            const float dr = __ldg(sh + gi), dp = __ldg(sh + 4 * lmx + gi);
+            const float dt = __ldg(sh + 4 * lmx + gi);
             u = __ldg(sh + lmx + gi);
             v = __ldg(sh + 2 * lmx + gi);
             wv = __ldg(sh + 3 * lmx + gi);
-            tp = (float)temp_dev(dr, dp);
+            tp = dt;
         }
         const int pj = L::pos(j);
         field_line32<LT, TL>(sm, 0, l)[pj] = u;
@@ -184,7 +182,7 @@ template <int AXIS, bool VISC>
 __device__ __forceinline__ void point_flux_mx(const float *__restrict__ sh, const float *__restrict__ g,
                                               int64_t lmx, int64_t gi, const Phys &ph, float (&flo)[5]) {
     const double dr = __ldg(sh + gi), u = __ldg(sh + lmx + gi), v = __ldg(sh + 2 * lmx + gi);
-    const double wv = __ldg(sh + 3 * lmx + gi), dp = __ldg(sh + 4 * lmx + gi);
+    const double wv = __ldg(sh + 3 * lmx + gi), dp = pres_dev(dr, __ldg(sh + 4 * lmx + gi));
     double gr[12];
     if (VISC) {
 #pragma unroll

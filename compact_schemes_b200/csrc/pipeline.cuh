@@ -313,7 +313,7 @@ k_grad_mx_pl(const double *__restrict__ q, float *__restrict__ sh, float *__rest
                     u = s5[1];
                     v = s5[2];
                     wv = s5[3];
-                    tp = (float)temp_dev(s5[0], s5[4]);
+                    tp = s5[4];
                     const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
                     double rr2 = 0.0;
 #pragma unroll
@@ -323,11 +323,11 @@ k_grad_mx_pl(const double *__restrict__ q, float *__restrict__ sh, float *__rest
                     m1 = fmax(m1, xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi));
                     m2 = fmax(m2, s.ri * ph.mu * ph.rr1 * ssi * ssi);
                 } else {
-                    const float dr = __ldg(sh + gi), dp = __ldg(sh + 4 * lmx + gi);
+                    const float dt = __ldg(sh + 4 * lmx + gi);
                     u = __ldg(sh + lmx + gi);
                     v = __ldg(sh + 2 * lmx + gi);
                     wv = __ldg(sh + 3 * lmx + gi);
-                    tp = (float)temp_dev(dr, dp);
+                    tp = dt;
                 }
                 const int pj = L::pos(j);
                 field_line32<LT, TL>(sm, 0, l)[pj] = u;
