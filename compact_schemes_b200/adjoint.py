@@ -121,3 +121,32 @@ def point_prim_vjp(q, pb):
     o = (ctypes.c_double * 5)()
     check(lib().cs_point_prim_vjp(_arr(q, 5), _arr(pb, 4), o))
     return list(o)
+
+
+def _main(argv=None):
+    """python -m compact_schemes_b200.adjoint --n N --steps K --every E: dJ/dq0
+    of the kinetic energy of the N^3 Taylor-Green box (profiling driver)."""
+    import argparse
+    import torch
+    from .solver import Solver, tgv_config, tgv_init
+    p = argparse.ArgumentParser()
+    p.add_argument("--n", type=int, default=64)
+    p.add_argument("--steps", type=int, default=4)
+    p.add_argument("--every", type=int, default=2)
+    a = p.parse_args(argv)
+    from compact_schemes_b200 import adjoint as A  # the package's classes, not __main__'s
+    cfg = tgv_config(a.n, use_graph=False)
+    s, adj = Solver(cfg), A.Adjoint(cfg)
+    q0 = torch.empty(5 * a.n ** 3, dtype=torch.float64, device="cuda")
+    tgv_init(q0, (a.n, a.n, a.n))
+    qr, dts = q0.clone(), []
+    for _ in range(a.steps):
+        s.step(qr)
+        dts.append(s.last_dt())
+    g = torch.empty_like(q0)
+    J = adj.gradient(q0, dts, a.every, g)
+    print("J", J, "|dJ/dq0|", float(g.norm()))
+
+
+if __name__ == "__main__":
+    _main()

@@ -408,6 +408,10 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         if (n < 5 || (s->ndf[0][a] && n < kLmd)) { delete s; return set_error(CS_ERR_UNSUPPORTED, "axis %d too short", a); }
         s->tab[a] = s->tables.get(n, kDeriv, s->ndf[0][a], s->ndf[1][a], 0.0);
         if (!s->tab[a]) { delete s; return CS_ERR_UNSUPPORTED; }
+        if (s->tab[a]->lt > 16) {
+            delete s;
+            return set_error(CS_ERR_UNSUPPORTED, "axis %d: the fused passes take lines of at most 512 points", a);
+        }
         s->active[a] = 1;
     }
     if (cfg->precision != CS_PREC_FP64 && cfg->precision != CS_PREC_MIXED) {

@@ -403,7 +403,6 @@ int launch_grad_tl(const PassArgs &a, const double *q, bool dtred, cudaStream_t 
         case 4: return launch_grad_t<4, AXIS, TL>(a, q, dtred, st);
         case 8: return launch_grad_t<8, AXIS, TL>(a, q, dtred, st);
         case 16: return launch_grad_t<16, AXIS, TL>(a, q, dtred, st);
-        case 32: return launch_grad_t<32, AXIS, TL>(a, q, dtred, st);
     }
     return set_error(CS_ERR_UNSUPPORTED, "chunk length");
 }
@@ -416,7 +415,6 @@ int launch_flux_tm(const PassArgs &a, const double *q, const double *qn, double 
         case 4: return launch_flux_t<4, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
         case 8: return launch_flux_t<8, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
         case 16: return launch_flux_t<16, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
-        case 32: return launch_flux_t<32, AXIS, TL, MODE>(a, q, qn, qout, drva, rk, st);
     }
     return set_error(CS_ERR_UNSUPPORTED, "chunk length");
 }

@@ -354,7 +354,6 @@ int launch_grad_mx_tl(const MixedArgs &a, const double *q, bool first, cudaStrea
         case 4: return launch_grad_mx_t<4, AXIS, TL>(a, q, first, st);
         case 8: return launch_grad_mx_t<8, AXIS, TL>(a, q, first, st);
         case 16: return launch_grad_mx_t<16, AXIS, TL>(a, q, first, st);
-        case 32: return launch_grad_mx_t<32, AXIS, TL>(a, q, first, st);
     }
     return set_error(CS_ERR_UNSUPPORTED, "chunk length");
 }
@@ -367,7 +366,6 @@ int launch_flux_mx_tm(const MixedArgs &a, const double *qn, double *qout, bool s
         case 4: return launch_flux_mx_t<4, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
         case 8: return launch_flux_mx_t<8, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
         case 16: return launch_flux_mx_t<16, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
-        case 32: return launch_flux_mx_t<32, AXIS, TL, MODE>(a, qn, qout, shadow_out, drva, rk, st);
     }
     return set_error(CS_ERR_UNSUPPORTED, "chunk length");
 }

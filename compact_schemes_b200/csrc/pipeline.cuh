@@ -531,7 +531,6 @@ int launch_flux_mx_pl_t(const MixedArgs &m, const double *qn, double *qout, bool
         case 4: return CALL(4);                                 \
         case 8: return CALL(8);                                 \
         case 16: return CALL(16);                               \
-        case 32: return CALL(32);                               \
     }                                                           \
     return set_error(CS_ERR_UNSUPPORTED, "chunk length");
 

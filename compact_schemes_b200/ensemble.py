@@ -154,3 +154,28 @@ def ensemble_tgv(boxes, cfl=0.5, viscous=True):
 
 def ensemble_points(boxes):
     return sum(math.prod(d) for d, _, _ in boxes)
+
+
+def _main(argv=None):
+    """python -m compact_schemes_b200.ensemble [--boxes B] [--steps K]: the
+    first B boxes of the seeded 64-box set, K ensemble steps (profiling driver)."""
+    import argparse
+    import torch
+    from .solver import tgv_init
+    p = argparse.ArgumentParser()
+    p.add_argument("--boxes", type=int, default=64)
+    p.add_argument("--steps", type=int, default=2)
+    a = p.parse_args(argv)
+    from compact_schemes_b200 import ensemble as E  # the package's classes, not __main__'s
+    boxes = E.draw_boxes(64, 0)[:a.boxes]
+    ens = E.Ensemble(E.ensemble_tgv(boxes))
+    q = torch.zeros(ens.state_size(), dtype=torch.float64, device="cuda")
+    for b, (d, m, _) in enumerate(boxes):
+        tgv_init(ens.box_view(q, b), d, m, 1e-4, b)
+    for _ in range(a.steps):
+        ens.step(q)
+    print("boxes", a.boxes, "points", ensemble_points(boxes), "dt[0]", ens.last_dt()[0])
+
+
+if __name__ == "__main__":
+    _main()

@@ -116,3 +116,27 @@ def tgv_init(q, dims, mach=0.1, noise=1e-4, seed=0, stream=None):
     lxi, let, lze = dims
     check(lib().cs_tgv_init(ptr(q), lxi, let, lze, float(mach), float(noise), int(seed),
                             stream_ptr(stream)))
+
+
+def _main(argv=None):
+    """python -m compact_schemes_b200.solver --n N [--precision P] [--steps K]:
+    K CFL-stepped RK steps of the N^3 Taylor-Green box (profiling driver)."""
+    import argparse
+    import torch
+    p = argparse.ArgumentParser()
+    p.add_argument("--n", type=int, default=128)
+    p.add_argument("--precision", type=int, default=PREC_FP64)
+    p.add_argument("--steps", type=int, default=1)
+    p.add_argument("--graph", type=int, default=0)
+    a = p.parse_args(argv)
+    from compact_schemes_b200 import solver as S  # the package's classes, not __main__'s
+    s = S.Solver(S.tgv_config(a.n, precision=a.precision, use_graph=bool(a.graph)))
+    q = torch.empty(5 * a.n ** 3, dtype=torch.float64, device="cuda")
+    S.tgv_init(q, (a.n, a.n, a.n))
+    for _ in range(a.steps):
+        s.step(q)
+    print("steps", a.steps, "last dt", s.last_dt())
+
+
+if __name__ == "__main__":
+    _main()
