@@ -73,6 +73,8 @@ def declare(L):
     L.cs_adjoint_create.argtypes = [pp, ctypes.POINTER(SolverConfig)]
     L.cs_adjoint_destroy.argtypes = [vp]
     L.cs_adjoint_deriv.argtypes = [vp, i32, i32, vp, vp, i32, i32, vp]
+    L.cs_adjoint_filter.argtypes = [vp, i32, i32, f64, vp, vp, i32, i32, vp]
+    L.cs_adjoint_filter.restype = i32
     L.cs_rhs_jvp.argtypes = [vp, vp, vp, vp, vp]
     L.cs_rhs_vjp.argtypes = [vp, vp, vp, vp, vp]
     L.cs_adjoint_stages.argtypes = [vp, vp, f64, pp, vp, vp]

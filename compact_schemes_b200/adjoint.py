@@ -37,6 +37,10 @@ class Adjoint:
         check(lib().cs_adjoint_deriv(self._h, int(axis), int(transpose), ptr(x), ptr(out), int(nfields),
                                      int(accumulate), stream_ptr(stream)))
 
+    def filter(self, axis, alpha_f, x, out, nfields=1, transpose=False, accumulate=False, stream=None):
+        check(lib().cs_adjoint_filter(self._h, int(axis), int(transpose), float(alpha_f), ptr(x), ptr(out),
+                                      int(nfields), int(accumulate), stream_ptr(stream)))
+
     def rhs_jvp(self, q, dq, out, stream=None):
         check(lib().cs_rhs_jvp(self._h, ptr(q), ptr(dq), ptr(out), stream_ptr(stream)))
 

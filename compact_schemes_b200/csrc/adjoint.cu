@@ -75,6 +75,43 @@ static int lines(cs_adjoint *a, int axis, bool trans, const double *in, int64_t 
     return CS_OK;
 }
 
+// The compact filter (Gaitonde-Visbal, filter_rhs) or its transpose along axis.
+static int filter_lines(cs_adjoint *a, int axis, bool trans, double af, const double *in, double *out, int nf,
+                        bool accum, cudaStream_t st) {
+    const int n = axis == 0 ? a->d.lxi : (axis == 1 ? a->d.let : a->d.lze);
+    const int nstart = a->ndf[0][axis], nend = a->ndf[1][axis];
+    const DeviceTables *t = a->tables.get(n, trans ? kFilterT : kFilter, nstart, nend, af);
+    if (!t) return CS_ERR_UNSUPPORTED;
+    const dim3 grid((unsigned)((a->F[axis] + 7) / 8), (unsigned)nf);
+    const int64_t lmx = a->lmx;
+#define CSB_FLINES(LT, AX)                                                                                      \
+    do {                                                                                                        \
+        if (trans)                                                                                              \
+            k_lines<LT, AX, true, true><<<grid, 256, 0, st>>>(in, lmx, out, lmx, accum, 1.0, t->t64, a->d.lxi,   \
+                                                              a->d.let, a->F[AX], nstart, nend, a->cf, af);     \
+        else                                                                                                    \
+            k_lines<LT, AX, false, true><<<grid, 256, 0, st>>>(in, lmx, out, lmx, accum, 1.0, t->t64, a->d.lxi,  \
+                                                               a->d.let, a->F[AX], nstart, nend, a->cf, af);    \
+    } while (0)
+#define CSB_FLINES_AX(LT)                       \
+    do {                                        \
+        if (axis == 0) CSB_FLINES(LT, 0);       \
+        else if (axis == 1) CSB_FLINES(LT, 1);  \
+        else CSB_FLINES(LT, 2);                 \
+    } while (0)
+    switch (t->lt) {
+        case 2: CSB_FLINES_AX(2); break;
+        case 4: CSB_FLINES_AX(4); break;
+        case 8: CSB_FLINES_AX(8); break;
+        case 16: CSB_FLINES_AX(16); break;
+        default: return set_error(CS_ERR_UNSUPPORTED, "adjoint: lines of more than 512 points");
+    }
+#undef CSB_FLINES_AX
+#undef CSB_FLINES
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
 static int grads(cs_adjoint *a, const double *q, cudaStream_t st) {
     for (int ax = 0; ax < 3; ++ax) {
         if (!a->active[ax]) continue;
@@ -230,6 +267,14 @@ int cs_adjoint_deriv(cs_adjoint *a, int axis, int transpose, const double *in, d
     if (!a->active[axis]) return set_error(CS_ERR_INVALID, "axis %d has a single point", axis);
     return lines(a, axis, transpose != 0, in, a->lmx, out, a->lmx, nfields, accumulate != 0, 1.0,
                  (cudaStream_t)stream);
+}
+
+int cs_adjoint_filter(cs_adjoint *a, int axis, int transpose, double alpha_f, const double *in, double *out,
+                      int nfields, int accumulate, void *stream) {
+    if (!a || !in || !out || axis < 0 || axis > 2 || nfields < 1) return set_error(CS_ERR_INVALID, "bad argument");
+    if (!a->active[axis]) return set_error(CS_ERR_INVALID, "axis %d has a single point", axis);
+    if (!(alpha_f > -0.5 && alpha_f < 0.5)) return set_error(CS_ERR_INVALID, "alpha_f %g outside (-1/2, 1/2)", alpha_f);
+    return filter_lines(a, axis, transpose != 0, alpha_f, in, out, nfields, accumulate != 0, (cudaStream_t)stream);
 }
 
 int cs_rhs_jvp(cs_adjoint *a, const double *q, const double *dq, double *dR, void *stream) {

@@ -58,13 +58,50 @@ __device__ __forceinline__ void stencil_t(const double *z, int n, int lane, int 
     }
 }
 
-// out[f] (=|+=) scale * D (or D^T) in[f] along AXIS, field f = blockIdx.y;
-// one warp per line, 8 lines per CTA.
-template <int LT, int AXIS, bool TRANS>
+// o = B_f^T z for the compact filter's right-hand side (filter_rhs): rows
+// i = j-3 .. j+3 contribute their coefficient at offset j - i; without
+// wrap-around, rows at distance 0, 1, 2 from an end use the identity, second-
+// and fourth-order stencils.
+template <int LT>
+__device__ __forceinline__ void filter_stencil_t(const double *z, int n, int lane, bool cyclic, double af,
+                                                 double (&o)[LT]) {
+    using L = LineLayout<LT>;
+    const double a60 = (11.0 + 10.0 * af) / 16.0, a61 = (15.0 + 34.0 * af) / 32.0;
+    const double a62 = (-3.0 + 6.0 * af) / 16.0, a63 = (1.0 - 2.0 * af) / 32.0;
+    const double a40 = (5.0 + 6.0 * af) / 8.0, a41 = (1.0 + 2.0 * af) / 2.0, a42 = (-1.0 + 2.0 * af) / 8.0;
+    const double a20 = (1.0 + 2.0 * af) / 2.0;
+#pragma unroll
+    for (int t = 0; t < LT; ++t) {
+        const int j = lane * LT + t;
+        double s = 0.0;
+        if (j < n) {
+#pragma unroll
+            for (int d = -3; d <= 3; ++d) {
+                int i = j + d;
+                if (cyclic) i = i < 0 ? i + n : (i >= n ? i - n : i);
+                else if (i < 0 || i >= n) continue;
+                const int o = d < 0 ? -d : d;  // |j - i|
+                const int dist = cyclic ? 3 : (i < n - 1 - i ? i : n - 1 - i);
+                double c;
+                if (dist >= 3) c = o == 0 ? a60 : (o == 1 ? 0.5 * a61 : (o == 2 ? 0.5 * a62 : 0.5 * a63));
+                else if (dist == 2) c = o == 0 ? a40 : (o == 1 ? 0.5 * a41 : (o == 2 ? 0.5 * a42 : 0.0));
+                else if (dist == 1) c = o == 0 ? a20 : (o == 1 ? 0.5 * a20 : 0.0);
+                else c = o == 0 ? 1.0 : 0.0;
+                s += c * z[L::pos(i)];
+            }
+        }
+        o[t] = s;
+    }
+}
+
+// out[f] (=|+=) scale * D (or D^T) in[f] along AXIS, field f = blockIdx.y, or
+// the compact filter (FILTER) and its transpose; one warp per line, 8 lines
+// per CTA.
+template <int LT, int AXIS, bool TRANS, bool FILTER = false>
 __global__ void __launch_bounds__(256) k_lines(const double *__restrict__ in, int64_t in_fs,
                                                double *__restrict__ out, int64_t out_fs, int accum, double scale,
                                                DevTables<double> tab, int lxi, int let, int64_t F, int nstart,
-                                               int nend, Coeffs cf) {
+                                               int nend, Coeffs cf, double af = 0.0) {
     constexpr int TL = 8;
     using L = LineLayout<LT>;
     __shared__ double sm[TL * L::kSlot];
@@ -80,7 +117,8 @@ __global__ void __launch_bounds__(256) k_lines(const double *__restrict__ in, in
         double *line = sm + w * L::kSlot;
         double d[1][LT];
         if (!TRANS) {
-            deriv_rhs<LT, double, double>(line, n, lane, nstart, nend, nullptr, cf, d[0]);
+            if (FILTER) filter_rhs<LT, double, double>(line, n, lane, tab.cyclic != 0, af, d[0]);
+            else deriv_rhs<LT, double, double>(line, n, lane, nstart, nend, nullptr, cf, d[0]);
             warp_solve<LT, 1, double>(tab, d, lane);
         } else {
 #pragma unroll
@@ -91,7 +129,8 @@ __global__ void __launch_bounds__(256) k_lines(const double *__restrict__ in, in
             for (int t = 0; t < LT; ++t)
                 if (lane * LT + t < n) line[L::pos_ct(lane, t)] = d[0][t];
             __syncwarp();
-            stencil_t<LT>(line, n, lane, nstart, nend, cf, d[0]);
+            if (FILTER) filter_stencil_t<LT>(line, n, lane, tab.cyclic != 0, af, d[0]);
+            else stencil_t<LT>(line, n, lane, nstart, nend, cf, d[0]);
         }
         __syncwarp();
 #pragma unroll

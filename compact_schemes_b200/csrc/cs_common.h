@@ -36,9 +36,9 @@ constexpr int kMaxLine = 1024;
 // six PCR steps (strides 1..32).
 constexpr int kPcrSteps = 6;
 
-// kDerivT: the transposed derivative matrix A^T of the left-hand side
-// (adjoint line solves).
-enum Scheme { kDeriv = 0, kFilter = 1, kDerivT = 2 };
+// kDerivT / kFilterT: the transposed left-hand-side matrices A^T (adjoint
+// line solves).
+enum Scheme { kDeriv = 0, kFilter = 1, kDerivT = 2, kFilterT = 3 };
 
 // Interface closure weights of the quasi-disjoint compact scheme
 // (numerics_base::deriv_setup, src/numerics_base.hpp:182-297).

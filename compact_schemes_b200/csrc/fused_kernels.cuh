@@ -29,6 +29,9 @@
 #ifndef CSB_SOLVE_GROUP
 #define CSB_SOLVE_GROUP 2
 #endif
+#ifndef CSB_GRAD_SOLVE_GROUP
+#define CSB_GRAD_SOLVE_GROUP CSB_SOLVE_GROUP
+#endif
 #ifndef CSB_RMW_CHUNK
 #define CSB_RMW_CHUNK 4     // points per chunk when only R is read back
 #endif
@@ -153,7 +156,7 @@ __device__ __forceinline__ void grad_tile(double *sm, int64_t line0, const doubl
     });
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
-    if (fidx < F) solve_fields<LT, TL, 4>(sm, w, lane, tab, nstart, nend, cf);
+    if (fidx < F) solve_fields<LT, TL, 4, CSB_GRAD_SOLVE_GROUP>(sm, w, lane, tab, nstart, nend, cf);
     tile_sync<AXIS, TL>();
     tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         const int pj = L::pos(j);

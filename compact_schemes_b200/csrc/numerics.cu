@@ -84,13 +84,20 @@ static bool host_tables_for(int n, int scheme, int nstart, int nend, double af, 
     } else {
         cyclic = nstart && nend;
         filter_rows(n, cyclic, af, a.data(), b.data(), c.data());
+        if (scheme == kFilterT && !cyclic) {  // the cyclic filter matrix is symmetric
+            std::vector<double> a0(a), c0(c);
+            for (int i = 0; i < n; ++i) {
+                a[i] = i > 0 ? c0[i - 1] : 0.0;
+                c[i] = i < n - 1 ? a0[i + 1] : 0.0;
+            }
+        }
     }
     return build_tables(n, a.data(), b.data(), c.data(), cyclic, h);
 }
 
 const DeviceTables *TableCache::get(int n, int scheme, int nstart, int nend, double af) {
     uint64_t bits = 0;
-    if (scheme == kFilter) std::memcpy(&bits, &af, sizeof bits);
+    if (scheme == kFilter || scheme == kFilterT) std::memcpy(&bits, &af, sizeof bits);
     TableKey key{n, scheme, nstart ? 1 : 0, nend ? 1 : 0, bits};
     std::lock_guard<std::mutex> lk(mu_);
     auto it = map_.find(key);

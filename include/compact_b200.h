@@ -329,6 +329,10 @@ int cs_adjoint_destroy(cs_adjoint *a);
 /* out[f] (= or +=) D_axis in[f] (transpose = 0) or D_axis^T in[f], f < nfields. */
 int cs_adjoint_deriv(cs_adjoint *a, int axis, int transpose, const double *in, double *out, int nfields,
                      int accumulate, void *stream);
+/* out[f] (= or +=) F_axis in[f] or F_axis^T in[f] for the compact filter of
+ * cs_filter (same alpha_f, the configuration's boundary codes). */
+int cs_adjoint_filter(cs_adjoint *a, int axis, int transpose, double alpha_f, const double *in, double *out,
+                      int nfields, int accumulate, void *stream);
 int cs_rhs_jvp(cs_adjoint *a, const double *q, const double *dq, double *dR, void *stream);
 int cs_rhs_vjp(cs_adjoint *a, const double *q, const double *lam, double *out, void *stream);
 /* Stage states of one step with time step dt: stages[0] = q^n (copied unless

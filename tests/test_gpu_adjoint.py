@@ -44,6 +44,27 @@ def test_transposed_derivative_dot_product(cuda, dims, nbc_code):
         assert abs(lhs - rhs) <= 1e-12 * float((y.abs() * Dx.abs()).sum()), (axis, lhs, rhs)
 
 
+@pytest.mark.parametrize("nbc_code", ["periodic", "physical"])
+@pytest.mark.parametrize("af", [0.0, 0.45, -0.3])
+def test_transposed_filter_dot_product_and_forward(cuda, nbc_code, af):
+    import compact_schemes_b200 as cs
+    b = cs.BC_PERIODIC if nbc_code == "periodic" else cs.BC_NON_REFLECTIVE
+    dims = (24, 40, 20)
+    _, _, a, _ = _setup(dims, nbc=[[b] * 3] * 2)
+    g = torch.Generator(device="cuda:0").manual_seed(8)
+    n = int(np.prod(dims))
+    x = torch.randn(n, dtype=torch.float64, device="cuda:0", generator=g)
+    y = torch.randn(n, dtype=torch.float64, device="cuda:0", generator=g)
+    nd = 1 if nbc_code == "periodic" else 0
+    for axis in range(3):
+        Fx, FTy = torch.empty_like(x), torch.empty_like(y)
+        a.filter(axis, af, x, Fx)
+        a.filter(axis, af, y, FTy, transpose=True)
+        assert abs(_dot(y, Fx) - _dot(FTy, x)) <= 1e-12 * float((y.abs() * Fx.abs()).sum()), axis
+        ref = O.filt(x.cpu().numpy(), dims, axis, nd, nd, alpha_f=af)
+        assert np.abs(Fx.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 def test_tangent_derivative_matches_oracle(cuda):
     dims = (24, 40, 20)
     _, _, a, _ = _setup(dims)
