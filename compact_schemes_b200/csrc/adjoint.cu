@@ -36,6 +36,10 @@ struct cs_adjoint {
     double *G = nullptr, *G2 = nullptr, *phi4 = nullptr, *F15 = nullptr, *qbar = nullptr;
     double *t1 = nullptr, *t2 = nullptr, *t3 = nullptr, *partial = nullptr;
     unsigned long long *dtacc = nullptr;
+    // non-reflective GCBC on the x faces: face mask, forward / tangent x-derivative
+    // terms at the faces [2][5][F], face adjoint of q, lambda for the x solve [5][lmx]
+    int gcbc_mask = 0;
+    double *rf = nullptr, *drf = nullptr, *qbf = nullptr, *lamx = nullptr;
 };
 
 namespace csb {
@@ -139,6 +143,20 @@ static int grads(cs_adjoint *a, const double *q, cudaStream_t st) {
     return CS_OK;
 }
 
+static unsigned face_blocks(const cs_adjoint *a) { return (unsigned)((2 * a->F[0] + 127) / 128); }
+
+// rf = (d/dxi F_x(q, G)) at the x faces; G must be current (viscous).
+static int gcbc_forward_faces(cs_adjoint *a, const double *q, cudaStream_t st) {
+    const int64_t lmx = a->lmx;
+    if (a->cfg.viscous) k_flux_x_eval<true><<<kPointBlocks, 256, 0, st>>>(q, a->G, a->F15, a->ap);
+    else k_flux_x_eval<false><<<kPointBlocks, 256, 0, st>>>(q, nullptr, a->F15, a->ap);
+    CSB_CUDA(cudaGetLastError());
+    if (int rc = lines(a, 0, false, a->F15, lmx, a->F15 + 5 * lmx, lmx, 5, false, 1.0, st)) return rc;
+    k_xface_extract<<<face_blocks(a), 128, 0, st>>>(a->F15 + 5 * lmx, a->rf, a->d.lxi, lmx, a->F[0]);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
 static int rhs_jvp(cs_adjoint *a, const double *q, const double *dq, double *dR, cudaStream_t st) {
     const int64_t lmx = a->lmx;
     const bool visc = a->cfg.viscous != 0;
@@ -158,9 +176,19 @@ static int rhs_jvp(cs_adjoint *a, const double *q, const double *dq, double *dR,
     for (int ax = 0; ax < 3; ++ax) {
         if (!a->active[ax]) continue;
         if (int rc = lines(a, ax, false, a->F15 + 5 * ax * lmx, lmx, dR, lmx, 5, !first, 1.0, st)) return rc;
+        if (ax == 0 && a->gcbc_mask) {
+            k_xface_extract<<<face_blocks(a), 128, 0, st>>>(dR, a->drf, a->d.lxi, lmx, a->F[0]);
+            CSB_CUDA(cudaGetLastError());
+        }
         first = false;
     }
     if (first) CSB_CUDA(cudaMemsetAsync(dR, 0, 5 * lmx * sizeof(double), st));
+    if (a->gcbc_mask) {
+        if (int rc = gcbc_forward_faces(a, q, st)) return rc;
+        k_gcbc_tan<<<face_blocks(a), 128, 0, st>>>(q, a->rf, dq, a->drf, dR, a->d.lxi, lmx, a->F[0], a->gcbc_mask,
+                                                   a->ap.ph);
+        CSB_CUDA(cudaGetLastError());
+    }
     return CS_OK;
 }
 
@@ -171,12 +199,27 @@ static int rhs_vjp(cs_adjoint *a, const double *q, const double *lam, double *ou
     const bool visc = a->cfg.viscous != 0;
     if (visc)
         if (int rc = grads(a, q, st)) return rc;
+    const double *lam_x = lam;
+    if (a->gcbc_mask) {
+        // the x-derivative term at the faces also feeds the GCBC correction
+        if (int rc = gcbc_forward_faces(a, q, st)) return rc;
+        CSB_CUDA(cudaMemcpyAsync(a->lamx, lam, 5 * lmx * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        k_gcbc_adj<<<face_blocks(a), 128, 0, st>>>(q, a->rf, lam, a->lamx, a->qbf, a->d.lxi, lmx, a->F[0],
+                                                   a->gcbc_mask, a->ap.ph);
+        CSB_CUDA(cudaGetLastError());
+        lam_x = a->lamx;
+    }
     for (int ax = 0; ax < 3; ++ax)
         if (a->active[ax])
-            if (int rc = lines(a, ax, true, lam, lmx, a->F15 + 5 * ax * lmx, lmx, 5, false, 1.0, st)) return rc;
+            if (int rc = lines(a, ax, true, ax == 0 ? lam_x : lam, lmx, a->F15 + 5 * ax * lmx, lmx, 5, false, 1.0, st))
+                return rc;
     if (visc) k_flux_adj<true><<<kPointBlocks, 256, 0, st>>>(q, a->G, a->F15, a->qbar, a->G2, a->ap, a->amask);
     else k_flux_adj<false><<<kPointBlocks, 256, 0, st>>>(q, nullptr, a->F15, a->qbar, nullptr, a->ap, a->amask);
     CSB_CUDA(cudaGetLastError());
+    if (a->gcbc_mask) {
+        k_xface_add<<<face_blocks(a), 128, 0, st>>>(a->qbf, a->qbar, a->d.lxi, lmx, a->F[0], a->gcbc_mask);
+        CSB_CUDA(cudaGetLastError());
+    }
     bool have_pb = false;
     if (visc) {
         for (int b = 0; b < 3; ++b) {
@@ -203,7 +246,9 @@ extern "C" {
 int cs_adjoint_destroy(cs_adjoint *a) {
     if (!a) return set_error(CS_ERR_INVALID, "null argument");
     if (a->fwd) cs_solver_destroy(a->fwd);
-    for (double *p : {a->G, a->G2, a->phi4, a->F15, a->qbar, a->t1, a->t2, a->t3, a->partial}) cudaFree(p);
+    for (double *p : {a->G, a->G2, a->phi4, a->F15, a->qbar, a->t1, a->t2, a->t3, a->partial, a->rf, a->drf, a->qbf,
+                      a->lamx})
+        cudaFree(p);
     cudaFree(a->dtacc);
     delete a;
     return CS_OK;
@@ -213,7 +258,6 @@ int cs_adjoint_create(cs_adjoint **out, const cs_solver_config *cfg) {
     if (!out || !cfg) return set_error(CS_ERR_INVALID, "null argument");
     *out = nullptr;
     if (cfg->precision != CS_PREC_FP64) return set_error(CS_ERR_UNSUPPORTED, "adjoint: FP64 only");
-    if (cfg->gcbc) return set_error(CS_ERR_UNSUPPORTED, "adjoint: characteristic boundary closure not linearized");
     auto *a = new cs_adjoint();
     a->cfg = *cfg;
     a->cfg.use_graph = 0;  // the stages run with per-step time steps
@@ -257,6 +301,16 @@ int cs_adjoint_create(cs_adjoint **out, const cs_solver_config *cfg) {
         return set_error(CS_ERR_ALLOC, "adjoint scratch allocation failed");
     }
     cudaMemset(a->G, 0, 12 * lmx * sizeof(double));
+    if (cfg->gcbc && a->active[0])
+        a->gcbc_mask = (cfg->nbc[0][0] == CS_BC_NON_REFLECTIVE ? 1 : 0) | (cfg->nbc[1][0] == CS_BC_NON_REFLECTIVE ? 2 : 0);
+    if (a->gcbc_mask) {
+        const size_t fb = 10 * a->F[0] * sizeof(double);
+        if (cudaMalloc(&a->rf, fb) != cudaSuccess || cudaMalloc(&a->drf, fb) != cudaSuccess ||
+            cudaMalloc(&a->qbf, fb) != cudaSuccess || !alloc(&a->lamx, 5)) {
+            cs_adjoint_destroy(a);
+            return set_error(CS_ERR_ALLOC, "adjoint face scratch allocation failed");
+        }
+    }
     *out = a;
     return CS_OK;
 }

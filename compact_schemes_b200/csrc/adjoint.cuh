@@ -262,3 +262,97 @@ __global__ void k_kinetic(const double *__restrict__ q, int64_t lmx, double dv, 
 }
 
 }  // namespace csb
+
+namespace csb {
+
+// F_x(q, G) at every point (the forward x flux; its x derivative at the
+// faces is what the GCBC correction reads).
+template <bool VISC>
+__global__ void k_flux_x_eval(const double *__restrict__ q, const double *__restrict__ G, double *__restrict__ Fx,
+                              AdjPoint ap) {
+    const int64_t lmx = ap.lmx;
+    CSB_GRID_STRIDE(i, lmx) {
+        double qq[5], g[12], o[5];
+        for (int m = 0; m < 5; ++m) qq[m] = q[m * lmx + i];
+        for (int k = 0; k < 12; ++k) g[k] = VISC ? G[k * lmx + i] : 0.0;
+        flux_eval<VISC>(0, qq, g, ap.ph, o);
+        for (int m = 0; m < 5; ++m) Fx[m * lmx + i] = o[m];
+    }
+}
+
+// face[(ip*5 + v)*F + fi] = src[v][point fi of face ip] (x faces)
+__global__ void k_xface_extract(const double *__restrict__ src, double *__restrict__ face, int lxi, int64_t lmx,
+                                int64_t F) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * F) return;
+    const int ip = (int)(t / F);
+    const int64_t fi = t % F, idx = fi * lxi + (ip ? lxi - 1 : 0);
+    for (int v = 0; v < 5; ++v) face[(int64_t)(ip * 5 + v) * F + fi] = src[v * lmx + idx];
+}
+
+// Tangent of the GCBC correction at the non-reflective x faces:
+// dR[face point] += d g(q, r)[dq, dr].
+__global__ void k_gcbc_tan(const double *__restrict__ q, const double *__restrict__ rf,
+                           const double *__restrict__ dq, const double *__restrict__ drf, double *__restrict__ dR,
+                           int lxi, int64_t lmx, int64_t F, int face_mask, PointPhys ph) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * F) return;
+    const int ip = (int)(t / F);
+    if (!((face_mask >> ip) & 1)) return;
+    const int64_t fi = t % F, idx = fi * lxi + (ip ? lxi - 1 : 0);
+    double c[3];
+    xface_normal(ph, c);
+    Dual qd[5], rd[5], o[5];
+    for (int v = 0; v < 5; ++v) {
+        qd[v] = dual(q[v * lmx + idx], dq[v * lmx + idx]);
+        rd[v] = dual(rf[(int64_t)(ip * 5 + v) * F + fi], drf[(int64_t)(ip * 5 + v) * F + fi]);
+    }
+    gcbc_point(qd, rd, c, ph, ip, o);
+    for (int v = 0; v < 5; ++v) dR[v * lmx + idx] += o[v].d;
+}
+
+// Adjoint of the GCBC correction: with the 5 x 10 Jacobian of g(q, r) at a
+// face point (ten dual evaluations), lam_x[face point] = lam + dg/dr^T lam
+// (the adjoint of the x-derivative term there) and qbf[face] = dg/dq^T lam.
+__global__ void k_gcbc_adj(const double *__restrict__ q, const double *__restrict__ rf,
+                           const double *__restrict__ lam, double *__restrict__ lam_x, double *__restrict__ qbf,
+                           int lxi, int64_t lmx, int64_t F, int face_mask, PointPhys ph) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * F) return;
+    const int ip = (int)(t / F);
+    if (!((face_mask >> ip) & 1)) return;
+    const int64_t fi = t % F, idx = fi * lxi + (ip ? lxi - 1 : 0);
+    double c[3];
+    xface_normal(ph, c);
+    double qv[5], rv[5], lv[5];
+    for (int v = 0; v < 5; ++v) {
+        qv[v] = q[v * lmx + idx];
+        rv[v] = rf[(int64_t)(ip * 5 + v) * F + fi];
+        lv[v] = lam[v * lmx + idx];
+    }
+    for (int k = 0; k < 10; ++k) {
+        Dual qd[5], rd[5], o[5];
+        for (int v = 0; v < 5; ++v) {
+            qd[v] = dual(qv[v], k == v ? 1.0 : 0.0);
+            rd[v] = dual(rv[v], k == 5 + v ? 1.0 : 0.0);
+        }
+        gcbc_point(qd, rd, c, ph, ip, o);
+        double s = 0.0;
+        for (int v = 0; v < 5; ++v) s += o[v].d * lv[v];
+        if (k < 5) qbf[(int64_t)(ip * 5 + k) * F + fi] = s;
+        else lam_x[(k - 5) * lmx + idx] = lv[k - 5] + s;
+    }
+}
+
+// qbar[face point] += qbf[face] on the faces of face_mask
+__global__ void k_xface_add(const double *__restrict__ qbf, double *__restrict__ qbar, int lxi, int64_t lmx,
+                            int64_t F, int face_mask) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * F) return;
+    const int ip = (int)(t / F);
+    if (!((face_mask >> ip) & 1)) return;
+    const int64_t fi = t % F, idx = fi * lxi + (ip ? lxi - 1 : 0);
+    for (int v = 0; v < 5; ++v) qbar[v * lmx + idx] += qbf[(int64_t)(ip * 5 + v) * F + fi];
+}
+
+}  // namespace csb

@@ -248,3 +248,73 @@ CSB_HD void flux_adj(int a, const double q[5], const double G[12], const double 
 #undef CSB_HD
 
 }  // namespace csb
+
+namespace csb {
+
+// Forward-mode dual number (value, one directional derivative) for the
+// face-local GCBC linearization.
+struct Dual {
+    double v, d;
+};
+__host__ __device__ __forceinline__ Dual dual(double v, double d = 0.0) { return Dual{v, d}; }
+__host__ __device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__host__ __device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__host__ __device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__host__ __device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__host__ __device__ __forceinline__ Dual operator*(double s, Dual a) { return {s * a.v, s * a.d}; }
+__host__ __device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+    const double iv = 1.0 / b.v;
+    return {a.v * iv, (a.d - a.v * iv * b.d) * iv};
+}
+__host__ __device__ __forceinline__ Dual dsqrt(Dual a) {
+    const double s = sqrt(a.v);
+    return {s, 0.5 * a.d / s};
+}
+
+// Non-reflective GCBC correction of the RHS at one x-face point (the
+// arithmetic of k_gcbc_x: characteristic amplitudes of the two acoustic waves
+// from r = d/dxi F_x at the point, incoming ones removed, mapped back to
+// conservative variables, scaled by 1/J), on dual numbers.  The wave
+// selection is taken from the values.
+__host__ __device__ __forceinline__ void gcbc_point(const Dual q[5], const Dual r[5], const double c[3],
+                                                    const PointPhys &ph, int ip, Dual out[5]) {
+    const Dual rho = q[0], rhoi = dual(1.0) / rho;
+    const Dual ve[3] = {q[1] * rhoi, q[2] * rhoi, q[3] * rhoi};
+    const Dual hv2 = 0.5 * (ve[0] * ve[0] + ve[1] * ve[1] + ve[2] * ve[2]);
+    const Dual pp = kGamm1 * (q[4] - rho * hv2);
+    const Dual ao = dsqrt(kGam * (rhoi * pp)), aoi = dual(1.0) / ao;
+    const Dual vn = c[0] * ve[0] + c[1] * ve[1] + c[2] * ve[2];
+    const double vs = c[0] * ph.umf[0] + c[1] * ph.umf[1] + c[2] * ph.umf[2];
+    Dual dr[5];
+    for (int v = 0; v < 5; ++v) dr[v] = ph.J * r[v];
+    const Dual ho = kGamm1 * (aoi * aoi), bo = dual(1.0) - ho * hv2, co = aoi * vn;
+    const Dual dm[3] = {c[0] * aoi, c[1] * aoi, c[2] * aoi};
+    const Dual rv[3] = {ho * ve[0], ho * ve[1], ho * ve[2]};
+    const Dual cha3 = (dual(1.0) - bo - co) * dr[0] + (dm[0] - rv[0]) * dr[1] + (dm[1] - rv[1]) * dr[2] +
+                      (dm[2] - rv[2]) * dr[3] + ho * dr[4];
+    const Dual cha4 = (dual(1.0) - bo + co) * dr[0] + (-dm[0] - rv[0]) * dr[1] + (-dm[1] - rv[1]) * dr[2] +
+                      (-dm[2] - rv[2]) * dr[3] + ho * dr[4];
+    const double ra0 = 1.0 - 2.0 * ip;
+    const Dual d3 = ra0 * (vn.v + vs + ao.v) > 0 ? -cha3 : dual(0.0);
+    const Dual d4 = ra0 * (vn.v + vs - ao.v) > 0 ? -cha4 : dual(0.0);
+    const Dual bo2 = hv2 + kHamm1 * (ao * ao), co2 = ao * vn;
+    const Dual em[3] = {c[0] * ao, c[1] * ao, c[2] * ao};
+    const double sb = 1.0 / ph.J;
+    out[0] = sb * (0.5 * d3 + 0.5 * d4);
+    for (int k = 0; k < 3; ++k) {
+        const Dual s3 = 0.5 * (ve[k] + em[k]);
+        out[1 + k] = sb * (s3 * d3 + (s3 - em[k]) * d4);
+    }
+    const Dual s3 = 0.5 * (bo2 + co2);
+    out[4] = sb * (s3 * d3 + (s3 - co2) * d4);
+}
+
+// Unit normal of the x faces from the metric row grad(xi).
+__host__ __device__ __forceinline__ void xface_normal(const PointPhys &ph, double c[3]) {
+    const double nrm = sqrt(ph.M[0][0] * ph.M[0][0] + ph.M[0][1] * ph.M[0][1] + ph.M[0][2] * ph.M[0][2]);
+    c[0] = ph.M[0][0] / nrm;
+    c[1] = ph.M[0][1] / nrm;
+    c[2] = ph.M[0][2] / nrm;
+}
+
+}  // namespace csb

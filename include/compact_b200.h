@@ -313,8 +313,9 @@ int cs_ensemble_autotune(cs_ensemble *e, const double *q, int reps, cs_ensemble_
 
 /* ---------------------------------------------------------------------------
  * Tangent-linear and adjoint of the RHS and of the RK step (no reference
- * counterpart).  For a cs_solver_config (FP64, no GCBC, lines of at most
- * 512 points), with dt held fixed:
+ * counterpart).  For a cs_solver_config (FP64, lines of at most 512 points;
+ * with gcbc set, the non-reflective x-face correction is linearized too),
+ * with dt held fixed:
  *   R'(q) dq    = sum_a D_a [dF_a/dq dq + dF_a/dG dG],   dG_b = D_b (dphi/dq dq)
  *   R'(q)^T l   = dF/dq^T mu + dphi/dq^T sum_b D_b^T (dF/dG^T mu)_b,   mu_a = D_a^T l
  * where D_a = A^-1 B is the compact derivative along axis a (its transpose is

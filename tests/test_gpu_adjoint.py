@@ -196,3 +196,30 @@ def test_multi_step_dot_product(cuda):
         lam = out
     lhs, rhs = _dot(y, dx), _dot(lam, x)
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+@pytest.mark.parametrize("viscous", [True, False])
+def test_gcbc_rhs_linearization(cuda, viscous):
+    """Non-reflective x faces with the GCBC correction: tangent against central
+    differences of the forward RHS (which applies the correction), adjoint
+    against tangent."""
+    import compact_schemes_b200 as cs
+    nbc = [[cs.BC_NON_REFLECTIVE, cs.BC_PERIODIC, cs.BC_PERIODIC]] * 2
+    dims = (32, 24, 20)
+    cfg = cs.tgv_config(None, dims=dims, mach=MACH, re=RE, nbc=nbc, gcbc=True, viscous=viscous, use_graph=False)
+    s, a = cs.Solver(cfg), cs.Adjoint(cfg)
+    q = torch.from_numpy(O.tgv_init(dims, MACH, 1e-4, 9)).to("cuda:0")
+    g = torch.Generator(device="cuda:0").manual_seed(10)
+    dq = torch.randn(q.shape, dtype=torch.float64, device="cuda:0", generator=g) * 1e-2
+    lam = torch.randn(q.shape, dtype=torch.float64, device="cuda:0", generator=g)
+    eps = 1e-5
+    rp, rm, t, v = (torch.empty_like(q) for _ in range(4))
+    s.rhs(q + eps * dq, rp)
+    s.rhs(q - eps * dq, rm)
+    a.rhs_jvp(q, dq, t)
+    fd = (rp - rm) / (2 * eps)
+    for m in range(5):
+        e = (t.view(5, -1)[m] - fd.view(5, -1)[m]).abs().max() / fd.view(5, -1)[m].abs().max()
+        assert e < 1e-6, (m, float(e))
+    a.rhs_vjp(q, lam, v)
+    assert abs(_dot(lam, t) - _dot(v, dq)) <= 1e-12 * float((lam.abs() * t.abs()).sum())
