@@ -59,6 +59,11 @@ struct HostTables {
     std::vector<double> fwd1, fwd2, bwd1, bwd2, rca, rcc, cycz;
     // reduced system: [step][row-in-lane][lane] and [row-in-lane][lane]
     std::vector<double> k1, k2, invb;
+    // PCR depth: the reduced system's couplings decay geometrically, so after
+    // pcr64 (pcr32) steps the remaining ones are below FP64 (FP32) resolution;
+    // invb / invb32 are the inverse diagonals after that many steps
+    int pcr64 = 6, pcr32 = 6;
+    std::vector<double> invb32;
 };
 
 // Choose the per-lane chunk length (power of two) for a line of n points.

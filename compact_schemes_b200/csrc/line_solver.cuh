@@ -32,6 +32,7 @@ struct DevTables {
     const CT *fwd1, *fwd2, *bwd1, *bwd2, *rca, *rcc, *k1, *k2, *invb, *cycz;
     CT cyc_s1, cyc_s2;
     int n, p, last_len, cyclic;
+    int pcr;  // PCR steps run on the reduced system (2..6)
 };
 
 // Shared-memory layout of one line: element j = c*LT + t lives at
@@ -99,6 +100,7 @@ __device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][L
     }
 #pragma unroll
     for (int s = 1; s < kPcrSteps; ++s) {
+        if (s >= T.pcr) break;
         const int dl = 1 << (s - 1);
         const CT ka = T.k1[s * 64 + lane], kb = T.k2[s * 64 + lane];
         const CT kc = T.k1[s * 64 + 32 + lane], kd = T.k2[s * 64 + 32 + lane];

@@ -182,6 +182,7 @@ extern "C" int cs_deriv_noalloc(int axis, const double *in, double *out, int nst
     tab.p = h.p;
     tab.last_len = h.last_len;
     tab.cyclic = 0;
+    tab.pcr = h.pcr64;
     Coeffs cf;
     compute_interface_coeffs(cf);
     const int64_t F = axis == 0 ? (int64_t)d.let * d.lze : (axis == 1 ? (int64_t)d.lxi * d.lze : (int64_t)d.lxi * d.let);

@@ -58,11 +58,14 @@ static void bind(DevTables<CT> &t, CT *base, const HostTables &h) {
     t.p = h.p;
     t.last_len = h.last_len;
     t.cyclic = h.cyclic ? 1 : 0;
+    t.pcr = sizeof(CT) == 4 ? h.pcr32 : h.pcr64;
 }
 
-static std::vector<double> pack(const HostTables &h) {
+// Device layout of the tables; fp32 selects the inverse diagonals of the
+// FP32 PCR depth.
+static std::vector<double> pack(const HostTables &h, bool fp32 = false) {
     std::vector<double> v;
-    for (auto *a : {&h.fwd1, &h.fwd2, &h.bwd1, &h.bwd2, &h.rca, &h.rcc, &h.k1, &h.k2, &h.invb})
+    for (auto *a : {&h.fwd1, &h.fwd2, &h.bwd1, &h.bwd2, &h.rca, &h.rcc, &h.k1, &h.k2, fp32 ? &h.invb32 : &h.invb})
         v.insert(v.end(), a->begin(), a->end());
     if (h.cyclic) v.insert(v.end(), h.cycz.begin(), h.cycz.end());
     else v.insert(v.end(), (size_t)h.lt * 32, 0.0);
@@ -109,7 +112,8 @@ const DeviceTables *TableCache::get(int n, int scheme, int nstart, int nend, dou
         return nullptr;
     }
     std::vector<double> v = pack(dt->host);
-    std::vector<float> vf(v.begin(), v.end());
+    const std::vector<double> v32 = pack(dt->host, true);
+    std::vector<float> vf(v32.begin(), v32.end());
     if (cudaMalloc(&dt->d64, v.size() * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&dt->d32, vf.size() * sizeof(float)) != cudaSuccess ||
         cudaMemcpy(dt->d64, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -573,13 +577,14 @@ int cs_filter(cs_numerics *nm, int axis, const double *in, double *out, double a
     }
 }
 
-int cs_line_tables(int n, int scheme, int nstart, int nend, double alpha_f, int meta[5],
+int cs_line_tables(int n, int scheme, int nstart, int nend, double alpha_f, int meta[7],
                    double *tables, size_t tables_len) {
     if (!meta) return set_error(CS_ERR_INVALID, "null meta");
     HostTables h;
     if (!host_tables_for(n, scheme, nstart, nend, alpha_f, h))
         return set_error(CS_ERR_UNSUPPORTED, "line length %d", n);
     meta[0] = h.n; meta[1] = h.lt; meta[2] = h.p; meta[3] = h.last_len; meta[4] = h.cyclic;
+    meta[5] = h.pcr64; meta[6] = h.pcr32;
     if (tables) {
         std::vector<double> v = pack(h);
         v.push_back(h.cyc_s1);

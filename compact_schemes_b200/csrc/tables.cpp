@@ -6,6 +6,7 @@
 // elimination factors, the coefficients of the 64-row reduced system's PCR
 // sweeps and, for cyclic systems, the Sherman-Morrison correction vector.
 // The device then only transforms right-hand sides.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -223,10 +224,32 @@ bool build_tables(int n, const double *a_in, const double *b_in, const double *c
             rc[2 * lane + 1] = C[len - 1];
         }
     }
-    // PCR on the 64-row reduced system; strides 1, 2, ..., 32.
+    // PCR on the 64-row reduced system; strides 1, 2, ..., 32.  The depth is
+    // the first step count after which every remaining coupling relative to
+    // its diagonal is below kPcrTol64 (kPcrTol32): dropping them then changes
+    // the solution by less than the arithmetic's own rounding.
+    constexpr double kPcrTol64 = 1e-20, kPcrTol32 = 1e-12;
     T.k1.assign(kPcrSteps * 2 * W, 0.0);
     T.k2.assign(kPcrSteps * 2 * W, 0.0);
     T.invb.assign(2 * W, 1.0);
+    T.invb32.assign(2 * W, 1.0);
+    T.pcr64 = T.pcr32 = kPcrSteps;
+    bool have64 = false, have32 = false;
+    auto record = [&](int steps) {
+        double res = 0.0;
+        for (int r = 0; r < 64; ++r) res = std::max(res, (std::fabs(ra[r]) + std::fabs(rc[r])) / std::fabs(rb[r]));
+        if (steps == kPcrSteps) res = 0.0;  // the full depth is exact
+        if (!have32 && res <= kPcrTol32) {
+            have32 = true;
+            T.pcr32 = steps;
+            for (int r = 0; r < 64; ++r) T.invb32[(size_t)(r & 1) * W + (r >> 1)] = 1.0 / rb[r];
+        }
+        if (!have64 && res <= kPcrTol64) {
+            have64 = true;
+            T.pcr64 = steps;
+            for (int r = 0; r < 64; ++r) T.invb[(size_t)(r & 1) * W + (r >> 1)] = 1.0 / rb[r];
+        }
+    };
     for (int st = 0; st < kPcrSteps; ++st) {
         const int sg = 1 << st;
         double na[64], nb[64], nc[64];
@@ -242,8 +265,9 @@ bool build_tables(int n, const double *a_in, const double *b_in, const double *c
         std::memcpy(ra, na, sizeof ra);
         std::memcpy(rb, nb, sizeof rb);
         std::memcpy(rc, nc, sizeof rc);
+        // the first step is always run (it couples each lane's two rows)
+        if (st >= 1) record(st + 1);
     }
-    for (int r = 0; r < 64; ++r) T.invb[(size_t)(r & 1) * W + (r >> 1)] = 1.0 / rb[r];
     return true;
 }
 

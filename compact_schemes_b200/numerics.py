@@ -124,7 +124,7 @@ class numerics_rtc(numerics_pc):  # noqa: N801
 def line_tables(n, scheme=0, nstart=0, nend=0, alpha_f=0.0):
     """Host copy of the line-solver tables (introspection for tests / autotuning)."""
     import numpy as np
-    meta = (ctypes.c_int * 5)()
+    meta = (ctypes.c_int * 7)()
     check(lib().cs_line_tables(n, scheme, nstart, nend, alpha_f, meta, None, 0))
     lt = meta[1]
     size = 7 * lt * 32 + 832 + 2
@@ -140,5 +140,5 @@ def line_tables(n, scheme=0, nstart=0, nend=0, alpha_f=0.0):
     out["invb"] = buf[o + 768:o + 832].reshape(2, 32)
     out["cycz"] = buf[o + 832:o + 832 + tl].reshape(lt, 32)
     out["s1"], out["s2"] = buf[-2], buf[-1]
-    out.update(n=meta[0], lt=lt, p=meta[2], last_len=meta[3], cyclic=bool(meta[4]))
+    out.update(n=meta[0], lt=lt, p=meta[2], last_len=meta[3], cyclic=bool(meta[4]), pcr64=meta[5], pcr32=meta[6])
     return out

@@ -130,10 +130,11 @@ int cs_filter(cs_numerics *nm, int axis, const double *in, double *out, double a
               cs_dcomp d, void *stream);
 
 /* Introspection of the line-solver tables (tests, autotuner): fills meta =
- * {n, lt, p, last_len, cyclic} and, if tables != NULL, the 6*lt*32 + 13*64 +
- * lt*32 doubles fwd1,fwd2,bwd1,bwd2,rca,rcc,k1,k2,invb,cycz,{s1,s2}.
+ * {n, lt, p, last_len, cyclic, pcr64, pcr32} (pcr*: PCR steps the FP64 / FP32
+ * solves run) and, if tables != NULL, the 6*lt*32 + 13*64 + lt*32 doubles
+ * fwd1,fwd2,bwd1,bwd2,rca,rcc,k1,k2,invb (FP64 depth),cycz,{s1,s2}.
  * scheme 0 = derivative (nstart/nend), 1 = filter (alpha_f). */
-int cs_line_tables(int n, int scheme, int nstart, int nend, double alpha_f, int meta[5],
+int cs_line_tables(int n, int scheme, int nstart, int nend, double alpha_f, int meta[7],
                    double *tables, size_t tables_len);
 
 /* ---------------------------------------------------------------------------

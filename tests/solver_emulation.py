@@ -1,7 +1,7 @@
 """Numpy emulation of the warp line solver (compact_schemes_b200/csrc/line_solver.cuh).
 
 Runs the exact sequence of operations one warp performs -- per-lane forward /
-backward elimination, the six PCR steps over "shuffles" (numpy rolls with
+backward elimination, the PCR steps over "shuffles" (numpy rolls with
 the shuffle's own-value behaviour at the warp edges), back substitution and
 the cyclic correction -- from the tables the library exports, so that the
 tables can be validated on a machine without a GPU.
@@ -34,7 +34,7 @@ def emulate(tab, r):
     n0 = y0 - k1[0, 0] * up(y1, 1) - k2[0, 0] * y1
     n1 = y1 - k1[0, 1] * y0 - k2[0, 1] * down(y0, 1)
     y0, y1 = n0, n1
-    for s in range(1, 6):
+    for s in range(1, tab.get("pcr64", 6)):
         dl = 1 << (s - 1)
         n0 = y0 - k1[s, 0] * up(y0, dl) - k2[s, 0] * down(y0, dl)
         n1 = y1 - k1[s, 1] * up(y1, dl) - k2[s, 1] * down(y1, dl)
