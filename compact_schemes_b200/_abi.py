@@ -95,6 +95,8 @@ def declare(L):
                  "cs_point_flux", "cs_point_flux_jvp", "cs_point_flux_vjp", "cs_point_prim", "cs_point_prim_jvp",
                  "cs_point_prim_vjp"):
         getattr(L, name).restype = i32
+    L.cs_solver_autotune.argtypes = [vp, vp, i32, ctypes.POINTER(ctypes.c_int * 3 * 2), vp]
+    L.cs_solver_autotune.restype = i32
     L.cs_solver_profile_begin.argtypes = [vp]
     L.cs_solver_profile_end.argtypes = [vp, vp, vp]
     for name in ("cs_solver_create", "cs_solver_destroy", "cs_solver_rhs", "cs_solver_stage",

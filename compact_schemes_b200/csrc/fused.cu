@@ -140,6 +140,7 @@ struct cs_solver {
     int64_t F[3] = {0, 0, 0};
     int tile[2][3] = {{8, 8, 8}, {8, 8, 16}};  // lines per tile: [gradient|flux][axis]
     int pl[2][3] = {{0, 0, 0}, {0, 0, 0}};     // pipelined kernels per [gradient|flux][axis]
+    int can[2][3] = {{0, 0, 0}, {0, 0, 0}};    // feasible schedules: 1 tile 8, 2 tile 16, 4 pipelined
     int nsm = 0;
     // optional per-pass event timing (eager path only)
     bool profiling = false;
@@ -458,6 +459,9 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
                                  2 * bytes(pl_tile_for(s->tab[a]->lt, elem == 4)));
             }
             s->pl[k][a] = cfg->schedule == CS_SCHED_PIPELINE && pl_fits;
+            s->can[k][a] = (bytes(8) <= (size_t)smem_max ? 1 : 0) |
+                           (a > 0 && !(elem == 4 && a == 1) && bytes(16) <= (size_t)smem_max ? 2 : 0) |
+                           (pl_fits ? 4 : 0);
             if (!s->pl[k][a] && bytes(s->tile[k][a]) > (size_t)smem_max) {
                 delete s;
                 return set_error(CS_ERR_UNSUPPORTED,
@@ -519,6 +523,66 @@ int cs_solver_profile_end(cs_solver *s, double ms[CS_PASS_KINDS], int launches[C
         ms[p.first] += t;
         launches[p.first] += 1;
     }
+    return CS_OK;
+}
+
+int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3], void *stream) {
+    if (!s || !q || reps < 1) return set_error(CS_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = (size_t)5 * s->d.lmx * sizeof(double);
+    double *scratch = nullptr;
+    if (cudaMalloc(&scratch, bytes) != cudaSuccess) return set_error(CS_ERR_ALLOC, "autotune scratch allocation failed");
+    const int saved_tile[2][3] = {{s->tile[0][0], s->tile[0][1], s->tile[0][2]},
+                                  {s->tile[1][0], s->tile[1][1], s->tile[1][2]}};
+    const int saved_pl[2][3] = {{s->pl[0][0], s->pl[0][1], s->pl[0][2]}, {s->pl[1][0], s->pl[1][1], s->pl[1][2]}};
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
+    // candidates, applied to every pass where feasible: tile 8, tile 16, pipelined
+    double best[2][3];
+    int pick[2][3];
+    for (int k = 0; k < 2; ++k)
+        for (int a = 0; a < 3; ++a) { best[k][a] = 1e300; pick[k][a] = 8; }
+    int rc = CS_OK;
+    double dt = 0.0;
+    CSB_CUDA(cudaMemcpyAsync(scratch, q, bytes, cudaMemcpyDeviceToDevice, st));
+    if ((rc = run_step(s, scratch, 0.0, st)) == CS_OK) {
+        CSB_CUDA(cudaStreamSynchronize(st));
+        cs_solver_last_dt(s, &dt);
+    }
+    for (int c = 0; c < 3 && rc == CS_OK && dt > 0.0; ++c) {
+        const int bit = 1 << c;
+        for (int k = 0; k < 2; ++k)
+            for (int a = 0; a < 3; ++a) {
+                const bool ok = (s->can[k][a] & bit) != 0;
+                s->pl[k][a] = ok && c == 2;
+                s->tile[k][a] = ok && c == 1 ? 16 : 8;
+                if (!(s->can[k][a] & 1) && !s->pl[k][a]) s->tile[k][a] = saved_tile[k][a];
+            }
+        cs_solver_profile_begin(s);
+        for (int r = 0; r < reps + 1 && rc == CS_OK; ++r) rc = run_step(s, scratch, dt, st);
+        double ms[kPassKinds];
+        int n[kPassKinds];
+        if (rc == CS_OK) rc = cs_solver_profile_end(s, ms, n);
+        if (rc) break;
+        for (int k = 0; k < 2; ++k)
+            for (int a = 0; a < 3; ++a) {
+                const int kind = (k == 0 ? kPassGradX : kPassFluxX) + a;
+                if (!(s->can[k][a] & bit) || !n[kind]) continue;
+                const double t = ms[kind] / n[kind];
+                if (t < best[k][a]) { best[k][a] = t; pick[k][a] = c == 2 ? 0 : (c == 1 ? 16 : 8); }
+            }
+    }
+    cudaFree(scratch);
+    if (rc || !(dt > 0.0)) {
+        for (int k = 0; k < 2; ++k)
+            for (int a = 0; a < 3; ++a) { s->tile[k][a] = saved_tile[k][a]; s->pl[k][a] = saved_pl[k][a]; }
+        return rc ? rc : set_error(CS_ERR_STATE, "autotune: no time step from the state");
+    }
+    for (int k = 0; k < 2; ++k)
+        for (int a = 0; a < 3; ++a) {
+            s->pl[k][a] = pick[k][a] == 0;
+            s->tile[k][a] = pick[k][a] == 0 ? 8 : pick[k][a];
+            if (choice) choice[k][a] = pick[k][a];
+        }
     return CS_OK;
 }
 

@@ -96,8 +96,12 @@ void compute_interface_coeffs(Coeffs &cf) {
         }
 }
 
+#ifndef CSB_MIN_CHUNK
+#define CSB_MIN_CHUNK 2
+#endif
+
 int chunk_length(int n) {
-    int lt = 2;
+    int lt = CSB_MIN_CHUNK;
     while (lt < 32 && (n + lt - 1) / lt > 32) lt *= 2;
     return lt;
 }

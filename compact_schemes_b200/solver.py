@@ -106,6 +106,13 @@ class Solver:
                                         ctypes.c_void_p(q_out.data_ptr()), float(dt),
                                         stream_ptr(stream)))
 
+    def autotune(self, q, reps=2, stream=None):
+        """Pick the fastest schedule per pass on a scratch copy of q; returns
+        {(kind, axis): 8 | 16 (one-phase tile lines) | 0 (pipelined)}."""
+        ch = (ctypes.c_int * 3 * 2)()
+        check(lib().cs_solver_autotune(self._h, ptr(q), int(reps), ctypes.byref(ch), stream_ptr(stream)))
+        return {(k, a): ch[k][a] for k in range(2) for a in range(3)}
+
     def last_dt(self):
         v = ctypes.c_double()
         check(lib().cs_solver_last_dt(self._h, ctypes.byref(v)))

@@ -262,6 +262,12 @@ int cs_solver_dt_device(cs_solver *s, double **dt_dev);
  * counts per pass kind: 0-2 gradient x/y/z, 3-5 flux x/y/z (z carries the RK
  * update), 6 GCBC. */
 #define CS_PASS_KINDS 7
+/* Autotuner: times `reps` eager steps of every feasible pass schedule (one-
+ * phase with 8- or 16-line tiles, pipelined) on a scratch copy of q (q is not
+ * modified) and keeps the fastest per pass; choice[kind][axis] (may be NULL)
+ * receives 8 or 16 (one-phase tile lines) or 0 (pipelined) for the gradient
+ * (kind 0) and flux (kind 1) passes.  Synchronizes. */
+int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3], void *stream);
 int cs_solver_profile_begin(cs_solver *s);
 int cs_solver_profile_end(cs_solver *s, double ms[CS_PASS_KINDS], int launches[CS_PASS_KINDS]);
 /* Taylor-Green initial state on a periodic [0,2pi)^3 grid in CANARD units

@@ -168,6 +168,25 @@ def test_pipelined_schedule_bit_identical(cuda, dims, gcbc, precision):
     assert torch.equal(outs[0][1], outs[1][1])
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_autotuned_schedule_bit_identical(cuda, precision):
+    """The autotuner only chooses among schedules that do the same arithmetic:
+    after tuning, steps equal an untuned solver's bit for bit."""
+    import torch
+    dims = (96, 64, 80)
+    q0 = O.tgv_init(dims, MACH, 1e-4, 12)
+    a, b = dev(q0), dev(q0)
+    s1, s2 = solver(dims, precision=precision), solver(dims, precision=precision)
+    choice = s2.autotune(b, reps=1)
+    assert set(choice.values()) <= {0, 8, 16}
+    assert torch.equal(b, dev(q0))  # tuning ran on a scratch copy
+    for _ in range(2):
+        s1.step(a)
+        s2.step(b)
+    torch.cuda.synchronize()
+    assert torch.equal(a.view(torch.int64), b.view(torch.int64))
+
+
 def test_100_steps_within_1e10(cuda):
     import torch
     dims = (32, 32, 32)
