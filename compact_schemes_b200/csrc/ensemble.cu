@@ -25,6 +25,7 @@ struct cs_ensemble {
     unsigned long long *dtacc = nullptr;
     double *dt = nullptr;
     int *ctl = nullptr;  // [0] error word, [1] queue head, [2..] done[nbox][kEnsPhases]
+    csb::Coeffs *cf_dev = nullptr;
     int lt_max = 2;
     int nsm = 1;
     cs_ensemble_tuning tune{0, 8, 0, 4};
@@ -132,6 +133,7 @@ static int ens_run_step(cs_ensemble *e, double *q, cudaStream_t st) {
     a.dtacc = e->dtacc;
     a.dt = e->dt;
     a.cf = e->cf;
+    a.cf_dev = e->cf_dev;
     a.chunk = e->tune.chunk;
     a.tile_doubles = ens_tile_doubles(e);
     const size_t smem = ens_smem(e);
@@ -142,8 +144,8 @@ static int ens_run_step(cs_ensemble *e, double *q, cudaStream_t st) {
         a.nitems = e->nitems[list];
         a.stage = k;
         CSB_CUDA(cudaMemsetAsync(e->ctl + 1, 0, sizeof(int) * (1 + kEnsPhases * e->nbox), st));
-        const int rc = e->tune.tile == 4 ? ens_launch_tl4(a, e->viscous, e->tune.ctas_per_sm, e->nsm, smem, st)
-                                         : ens_launch_tl8(a, e->viscous, e->tune.ctas_per_sm, e->nsm, smem, st);
+        const int rc = e->tune.tile == 4 ? ens_launch_tl4(a, e->viscous, e->tune.ctas_per_sm, e->nsm, smem, st, e->nbox)
+                                         : ens_launch_tl8(a, e->viscous, e->tune.ctas_per_sm, e->nsm, smem, st, e->nbox);
         if (rc) return rc;
     }
     return CS_OK;
@@ -178,12 +180,15 @@ int cs_ensemble_destroy(cs_ensemble *e) {
     cudaFree(e->dtacc);
     cudaFree(e->dt);
     cudaFree(e->ctl);
+    cudaFree(e->cf_dev);
     delete e;
     return CS_OK;
 }
 
 int cs_ensemble_create(cs_ensemble **out, int nbox, const cs_solver_config *boxes) {
     if (!out || !boxes || nbox < 1) return set_error(CS_ERR_INVALID, "null argument or no boxes");
+    if (nbox > kEnsMaxBoxes)
+        return set_error(CS_ERR_UNSUPPORTED, "ensemble of %d boxes: at most %d per ensemble", nbox, kEnsMaxBoxes);
     *out = nullptr;
     auto *e = new cs_ensemble();
     e->nbox = nbox;
@@ -244,12 +249,14 @@ int cs_ensemble_create(cs_ensemble **out, int nbox, const cs_solver_config *boxe
                     cudaMalloc(&e->rhs, e->nr * sizeof(double)) == cudaSuccess &&
                     cudaMalloc(&e->dtacc, 2 * nbox * sizeof(unsigned long long)) == cudaSuccess &&
                     cudaMalloc(&e->dt, nbox * sizeof(double)) == cudaSuccess &&
-                    cudaMalloc(&e->ctl, (2 + kEnsPhases * nbox) * sizeof(int)) == cudaSuccess;
+                    cudaMalloc(&e->ctl, (2 + kEnsPhases * nbox) * sizeof(int)) == cudaSuccess &&
+                    cudaMalloc(&e->cf_dev, sizeof(Coeffs)) == cudaSuccess;
     if (!ok) {
         cs_ensemble_destroy(e);
         return set_error(CS_ERR_ALLOC, "ensemble scratch allocation failed");
     }
     cudaMemcpy(e->dbox, e->hbox.data(), nbox * sizeof(EnsBox), cudaMemcpyHostToDevice);
+    cudaMemcpy(e->cf_dev, &e->cf, sizeof(Coeffs), cudaMemcpyHostToDevice);
     cudaMemset(e->grad, 0, e->ng * sizeof(double));
     cudaMemset(e->dt, 0, nbox * sizeof(double));
     cudaMemset(e->ctl, 0, (2 + kEnsPhases * nbox) * sizeof(int));

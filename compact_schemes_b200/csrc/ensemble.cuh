@@ -69,6 +69,7 @@ struct EnsArgs {
     unsigned long long *dtacc;  // [nbox][2] CFL maxima
     double *dt;      // [nbox] dt of the step
     Coeffs cf;
+    const Coeffs *cf_dev;  // device copy of cf (source of the constant copy)
     int stage;       // 0..3
     int chunk;       // tiles per work item
     int tile_doubles;  // shared memory of the tile buffer (the segment starts follow it)
@@ -77,9 +78,21 @@ struct EnsArgs {
 // One work item of pass KIND for chunk length LT.  Each (KIND, LT) body is its
 // own function: the registers of one pass do not have to coexist with those of
 // the others.
+// The box descriptors of the launch live in constant memory (one copy per
+// translation unit, refreshed from the ensemble's device table before every
+// stage launch): the compiler may then reload a parameter instead of keeping
+// it in a register, since constant memory cannot change during the launch.
+constexpr int kEnsMaxBoxes = 96;
+static __constant__ EnsBox c_ens_boxes[kEnsMaxBoxes];
+static __constant__ Coeffs c_ens_cf;
+
+// Points per read-modify-write chunk in the ensemble's flux items (fewer than
+// the per-box passes: the items have fewer registers to spare).
+constexpr int kEnsRmwChunk = 2, kEnsRmwChunkRk = 1;
+
 template <int TL, bool VISC, int LT, int KIND>
 __device__ __noinline__ void ens_item(const EnsArgs &a, int b, int64_t line0, double *sm) {
-    const EnsBox &bx = a.boxes[b];
+    const EnsBox &bx = c_ens_boxes[b];
     const int stage = a.stage;
     const double *qin = (stage == 0 ? a.q : a.q1) + bx.qoff;
     double *g = a.grad + bx.goff;
@@ -89,10 +102,10 @@ __device__ __noinline__ void ens_item(const EnsArgs &a, int b, int64_t line0, do
     if (KIND < 3) {
         if (KIND == 0 && stage == 0)
             grad_tile<LT, 0, TL, true>(sm, line0, qin, g, tab, bx.lxi, bx.let, bx.lmx, bx.F[0], bx.nstart[0],
-                                       bx.nend[0], a.cf, ph, a.dtacc + 2 * b);
+                                       bx.nend[0], c_ens_cf, ph, a.dtacc + 2 * b);
         else
             grad_tile<LT, AX, TL, false>(sm, line0, qin, g + 4 * AX * bx.lmx, tab, bx.lxi, bx.let, bx.lmx,
-                                         bx.F[AX], bx.nstart[AX], bx.nend[AX], a.cf, ph, nullptr);
+                                         bx.F[AX], bx.nstart[AX], bx.nend[AX], c_ens_cf, ph, nullptr);
         return;
     }
     double *rhs = a.rhs + bx.roff;
@@ -107,8 +120,9 @@ __device__ __noinline__ void ens_item(const EnsArgs &a, int b, int64_t line0, do
     const double *qn = a.q + bx.qoff;
     double *qout = (stage == 3 ? a.q : a.q1) + bx.qoff;
     constexpr int MODE = KIND == 3 ? kWrite : (KIND == 4 ? kAccum : kAccumRk);
-    flux_tile<LT, AX, TL, MODE, VISC, true>(sm, line0, qin, g, rhs, qn, qout, nullptr, tab, bx.lxi, bx.let,
-                                            bx.lmx, bx.F[AX], bx.nstart[AX], bx.nend[AX], a.cf, ph, rk);
+    constexpr int P = MODE == kAccum ? kEnsRmwChunk : kEnsRmwChunkRk;
+    flux_tile<LT, AX, TL, MODE, VISC, true, P>(sm, line0, qin, g, rhs, qn, qout, nullptr, tab, bx.lxi, bx.let,
+                                               bx.lmx, bx.F[AX], bx.nstart[AX], bx.nend[AX], c_ens_cf, ph, rk);
 }
 
 template <int TL, bool VISC, int LT>
@@ -125,7 +139,7 @@ __device__ __forceinline__ void ens_run_lt(const EnsArgs &a, int b, int kind, in
 
 template <int TL, bool VISC>
 __device__ __forceinline__ void ens_run_item(const EnsArgs &a, int b, int kind, int64_t line0, double *sm) {
-    const int lt = a.boxes[b].lt[kind % 3];
+    const int lt = c_ens_boxes[b].lt[kind % 3];
     if (lt == 2) ens_run_lt<TL, VISC, 2>(a, b, kind, line0, sm);
     else if (lt == 4) ens_run_lt<TL, VISC, 4>(a, b, kind, line0, sm);
     else ens_run_lt<TL, VISC, 8>(a, b, kind, line0, sm);
@@ -199,7 +213,11 @@ namespace csb {
 // Launch one stage of the ensemble with TL-line work items: ctas_per_sm
 // resident CTAs per SM (0: as many as fit), at most one CTA per item.
 template <int TL>
-int ens_launch_t(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t smem, cudaStream_t st) {
+int ens_launch_t(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t smem, cudaStream_t st, int nbox) {
+    // this translation unit's constant copy of the box table (stream-ordered)
+    CSB_CUDA(cudaMemcpyToSymbolAsync(c_ens_boxes, a.boxes, (size_t)nbox * sizeof(EnsBox), 0,
+                                     cudaMemcpyDeviceToDevice, st));
+    CSB_CUDA(cudaMemcpyToSymbolAsync(c_ens_cf, a.cf_dev, sizeof(Coeffs), 0, cudaMemcpyDeviceToDevice, st));
     auto kern = visc ? k_ensemble_stage<TL, true> : k_ensemble_stage<TL, false>;
     if (int rc = set_smem(kern, smem)) return rc;
     int nb = 0;
@@ -215,7 +233,7 @@ int ens_launch_t(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t s
 }
 
 // ensemble_tl4.cu / ensemble_tl8.cu
-int ens_launch_tl4(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t smem, cudaStream_t st);
-int ens_launch_tl8(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t smem, cudaStream_t st);
+int ens_launch_tl4(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t smem, cudaStream_t st, int nbox);
+int ens_launch_tl8(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t smem, cudaStream_t st, int nbox);
 
 }  // namespace csb

@@ -3,8 +3,8 @@
 
 namespace csb {
 
-int ens_launch_tl8(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t smem, cudaStream_t st) {
-    return ens_launch_t<8>(a, visc, ctas_per_sm, nsm, smem, st);
+int ens_launch_tl8(const EnsArgs &a, bool visc, int ctas_per_sm, int nsm, size_t smem, cudaStream_t st, int nbox) {
+    return ens_launch_t<8>(a, visc, ctas_per_sm, nsm, smem, st, nbox);
 }
 
 }  // namespace csb

@@ -248,7 +248,8 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
 // One tile of the flux pass (TL * 32 threads; sm holds 5 * TL line slots).
 // CG: the RHS accumulator, gradients and CFL maxima come from other CTAs of
 // the same launch (ensemble) and are read from L2.
-template <int LT, int AXIS, int TL, int MODE, bool VISC, bool CG = false>
+template <int LT, int AXIS, int TL, int MODE, bool VISC, bool CG = false,
+          int P = MODE == kAccum ? CSB_RMW_CHUNK : CSB_RMW_CHUNK_RK>
 __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const double *__restrict__ q,
                                           const double *__restrict__ g, double *__restrict__ rhs,
                                           const double *__restrict__ qn, double *__restrict__ qout,
@@ -293,8 +294,7 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
             for (int m = 0; m < 5; ++m) rhs[m * lmx + gi] = field_line<LT, TL>(sm, m, l)[pj];
         });
     } else {
-        // read-modify-write: all loads of a chunk first
-        constexpr int P = MODE == kAccum ? CSB_RMW_CHUNK : CSB_RMW_CHUNK_RK;
+        // read-modify-write: all loads of a chunk of P points first
         double rv[P][5], qv[P][5];
         tile_for_each_chunked<AXIS, TL, P>(
             line0, F, n, lxi, let,

@@ -286,7 +286,10 @@ int cs_tgv_init(double *q, int lxi, int let, int lze, double mach, double noise_
  * arithmetic is that of cs_solver_step with a CFL time step, so every box's
  * result is bit-identical to stepping it with its own cs_solver.
  * The state of all boxes is one packed device array: box b's q [5][lmx_b]
- * starts at cs_ensemble_box_offset(b).
+ * starts at cs_ensemble_box_offset(b).  At most 96 boxes per ensemble; the
+ * stage kernel reads the box table from constant memory that every ensemble
+ * of a device shares, so ensembles on one device step one at a time (steps
+ * issued on one stream, or synchronized between streams).
  * ------------------------------------------------------------------------- */
 typedef struct cs_ensemble cs_ensemble;
 
