@@ -75,9 +75,6 @@ struct EnsArgs {
     int tile_doubles;  // shared memory of the tile buffer (the segment starts follow it)
 };
 
-// One work item of pass KIND for chunk length LT.  Each (KIND, LT) body is its
-// own function: the registers of one pass do not have to coexist with those of
-// the others.
 // The box descriptors of the launch live in constant memory (one copy per
 // translation unit, refreshed from the ensemble's device table before every
 // stage launch): the compiler may then reload a parameter instead of keeping
@@ -90,8 +87,11 @@ static __constant__ Coeffs c_ens_cf;
 // the per-box passes: the items have fewer registers to spare).
 constexpr int kEnsRmwChunk = 2, kEnsRmwChunkRk = 1;
 
+// One work item of pass KIND for chunk length LT, inlined into the stage
+// kernel (with the box parameters in constant memory the combined body spills
+// little; separate functions measured slower by their call overhead).
 template <int TL, bool VISC, int LT, int KIND>
-__device__ __noinline__ void ens_item(const EnsArgs &a, int b, int64_t line0, double *sm) {
+__device__ __forceinline__ void ens_item(const EnsArgs &a, int b, int64_t line0, double *sm) {
     const EnsBox &bx = c_ens_boxes[b];
     const int stage = a.stage;
     const double *qin = (stage == 0 ? a.q : a.q1) + bx.qoff;
