@@ -156,7 +156,7 @@ __device__ __forceinline__ void grad_tile(double *sm, int64_t line0, const doubl
     });
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
-    if (fidx < F) solve_fields<LT, TL, 4, CSB_GRAD_SOLVE_GROUP>(sm, w, lane, tab, nstart, nend, cf);
+    if (fidx < F) solve_fields<LT, TL, 4, (LT >= 16 ? 1 : CSB_GRAD_SOLVE_GROUP)>(sm, w, lane, tab, nstart, nend, cf);
     tile_sync<AXIS, TL>();
     tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         const int pj = L::pos(j);
@@ -249,7 +249,7 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
 // CG: the RHS accumulator, gradients and CFL maxima come from other CTAs of
 // the same launch (ensemble) and are read from L2.
 template <int LT, int AXIS, int TL, int MODE, bool VISC, bool CG = false,
-          int P = MODE == kAccum ? CSB_RMW_CHUNK : CSB_RMW_CHUNK_RK>
+          int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK)>
 __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const double *__restrict__ q,
                                           const double *__restrict__ g, double *__restrict__ rhs,
                                           const double *__restrict__ qn, double *__restrict__ qout,
@@ -269,7 +269,7 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
     if (fidx < F) {
-        solve_fields<LT, TL, 5>(sm, w, lane, tab, nstart, nend, cf);
+        solve_fields<LT, TL, 5, (LT >= 16 ? 1 : CSB_SOLVE_GROUP)>(sm, w, lane, tab, nstart, nend, cf);
         if (drva) {
             // line-end derivatives for the characteristic boundary closure
             // (drva of deriv_kernel_2d, src/cuda/kernels/numerics_pc.hpp:237-248)

@@ -49,11 +49,14 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
                                               int nend, const Coeffs &cf, int refine) {
     const int n = tab.n;
     const int len = lane_len(lane, LT, tab.p, tab.last_len);
-    double r64[LT];
-    deriv_rhs<LT, double, float>(line, n, lane, nstart, nend, nullptr, cf, r64);
-    float x[1][LT];
+    // right-hand side formed in FP64 (its differences cancel), rounded once
+    float r32[LT], x[1][LT];
+    {
+        double r64[LT];
+        deriv_rhs<LT, double, float>(line, n, lane, nstart, nend, nullptr, cf, r64);
 #pragma unroll
-    for (int t = 0; t < LT; ++t) x[0][t] = (float)r64[t];
+        for (int t = 0; t < LT; ++t) x[0][t] = r32[t] = (float)r64[t];
+    }
     warp_solve<LT, 1, float>(tab, x, lane);
     if (refine) {
         const float xm0 = __shfl_up_sync(0xffffffffu, x[0][LT - 1], 1);
@@ -69,7 +72,7 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
 #pragma unroll
             for (int u = 0; u + 1 < LT; ++u)
                 if (u == t && t + 1 < len) xp = (double)x[0][u + 1];
-            const double res = r64[t] - (a * xm + (double)x[0][t] + cc * xp);
+            const double res = (double)r32[t] - (a * xm + (double)x[0][t] + cc * xp);
             e[0][t] = j < n ? (float)res : 0.0f;
         }
         warp_solve<LT, 1, float>(tab, e, lane);
@@ -270,7 +273,7 @@ k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__re
             for (int m = 0; m < 5; ++m) rhs[m * lmx + gi] = field_line32<LT, TL>(sm, m, l)[pj];
         });
     } else {
-        constexpr int P = MODE == kAccum ? CSB_RMW_CHUNK : CSB_RMW_CHUNK_RK;
+        constexpr int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK);
         float rv[P][5];
         double qv[P][5];
         tile_for_each_chunked<AXIS, TL, P>(
