@@ -88,6 +88,6 @@ def nbc_array(nbc):
 
 from .numerics import numerics_pc, numerics_rtc  # noqa: E402,F401
 from .solver import Solver, SolverConfig, tgv_config, tgv_init  # noqa: E402,F401
-from .physics import physics, physics_rtc, gcbc_go, thermo, rk_update  # noqa: E402,F401
+from .physics import physics, physics_rtc, gcbc_go, thermo, rk_update, wall_condition_update  # noqa: E402,F401
 from .ensemble import Ensemble, draw_boxes, ensemble_tgv  # noqa: E402,F401
 from .adjoint import Adjoint  # noqa: E402,F401

@@ -38,6 +38,8 @@ def declare(L):
     L.cs_calc_time_step.argtypes = [vp, vp, vp, vp, vp, vp, vp, f64, ctypes.POINTER(f64), sz, vp]
     L.cs_gcbc_go.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, Dcomp, vp, vp]
     L.cs_thermo.argtypes = [vp, vp, vp, sz, vp]
+    L.cs_wall_condition_update.argtypes = [vp, vp, ctypes.POINTER(f64), Dcomp, vp, vp]
+    L.cs_wall_condition_update.restype = i32
     L.cs_rk_update.argtypes = [vp, vp, vp, f64, vp, sz, vp]
     for name in ("cs_physics_create", "cs_physics_destroy", "cs_physics_set_umf", "cs_physics_buffers",
                  "cs_calc_fluxes_pre", "cs_calc_fluxes", "cs_calc_viscous_shear_stress",

@@ -284,6 +284,33 @@ inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t
 
 using namespace csb;
 
+// Wall boundary state update at one face plane (wall_inviscid_kernel /
+// wall_viscous_kernel, src/cuda/kernels/gcbc.hpp:160-249): points with
+// npex == 0 get, inviscid, rho E = rho^gamma / (gamma (gamma-1)) + |m|^2 / (2 rho)
+// (isentropic pressure, momentum kept); viscous, m = -rho umf and
+// rho E = rho / (gamma (gamma-1)) + |m|^2 / (2 rho) with the updated m
+// (isothermal wall, T = 1).  plane = ip * (n - 1).
+__global__ void k_wall_face(double *__restrict__ q, const int *__restrict__ npex, double u0, double u1, double u2,
+                            int lxi, int let, int64_t lmx, int axis, int plane, int viscous, int64_t nf) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nf) return;
+    int64_t idx;
+    if (axis == 0) idx = plane + (int64_t)lxi * t;                                   // t = j + let k
+    else if (axis == 1) idx = t % lxi + (int64_t)lxi * (plane + (int64_t)let * (t / lxi));  // t = i + lxi k
+    else idx = t + (int64_t)lxi * let * plane;                                       // t = i + lxi j
+    if (npex[idx] != 0) return;
+    const double hamhamm1 = (1.0 / kGam) * kHamm1;
+    const double rho = q[idx];
+    if (viscous) {
+        q[lmx + idx] = -rho * u0;
+        q[2 * lmx + idx] = -rho * u1;
+        q[3 * lmx + idx] = -rho * u2;
+    }
+    const double m1 = q[lmx + idx], m2 = q[2 * lmx + idx], m3 = q[3 * lmx + idx];
+    const double ke = 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / rho;
+    q[4 * lmx + idx] = (viscous ? hamhamm1 * rho : hamhamm1 * pow(rho, kGam)) + ke;
+}
+
 extern "C" {
 
 int cs_physics_create(cs_physics **out, cs_dcomp d, int viscous) {
@@ -426,6 +453,24 @@ int cs_calc_time_step(cs_physics *ph, const double *xim, const double *etm, cons
     CSB_CUDA(cudaStreamSynchronize(st));
     const double a = cfl / h[0], b = 0.5 / h[1];
     *dte = a < b ? a : b;
+    return CS_OK;
+}
+
+int cs_wall_condition_update(double *q, const int *npex, const double umf[3], cs_dcomp d, const int nbc[2][3],
+                             void *stream) {
+    if (!q || !npex || !umf || !nbc) return set_error(CS_ERR_INVALID, "null argument");
+    if (d.lxi < 1 || d.let < 1 || d.lze < 1 || d.lmx != d.lxi * d.let * d.lze) return set_error(CS_ERR_INVALID, "dims");
+    const int dims[3] = {d.lxi, d.let, d.lze};
+    for (int a = 0; a < 3; ++a)
+        for (int ip = 0; ip < 2; ++ip) {
+            const int code = nbc[ip][a];
+            if (code != CS_BC_WALL_INVISCID && code != CS_BC_WALL_VISCOUS) continue;
+            const int64_t nf = (int64_t)d.lmx / dims[a];
+            k_wall_face<<<blocks_for(nf, 256), 256, 0, (cudaStream_t)stream>>>(
+                q, npex, umf[0], umf[1], umf[2], d.lxi, d.let, d.lmx, a, ip * (dims[a] - 1),
+                code == CS_BC_WALL_VISCOUS ? 1 : 0, nf);
+            CSB_CUDA(cudaGetLastError());
+        }
     return CS_OK;
 }
 

@@ -84,6 +84,14 @@ class physics:  # noqa: N801 - reference class name
 physics_rtc = physics
 
 
+def wall_condition_update(q, npex, dims, nbc, umf=(0.0, 0.0, 0.0), stream=None):
+    """wall_condition_update (src/gcbc.hpp:188-228) on a device state q [5*lmx]
+    with the int32 wall mask npex [lmx] (0 = wall point)."""
+    from . import Dcomp, nbc_array
+    u = (ctypes.c_double * 3)(*[float(x) for x in umf])
+    check(lib().cs_wall_condition_update(ptr(q), ptr(npex), u, Dcomp.of(*dims), nbc_array(nbc), stream_ptr(stream)))
+
+
 def thermo(q, de, pressure, stream=None):
     check(lib().cs_thermo(ptr(q), ptr(de), ptr(pressure), pressure.numel(), stream_ptr(stream)))
 

@@ -179,6 +179,14 @@ int cs_calc_time_step(cs_physics *ph, const double *xim, const double *etm, cons
  * (driver/canard.cu:142-143): de0 = 1/rho, de1..3 = u, v, w,
  * de4 = gamma p / rho (T in CANARD units, rho_inf = c_inf = 1), p. */
 int cs_thermo(const double *q, double *de, double *p, size_t n, void *stream);
+/* Wall boundary state update, wall_condition_update (src/gcbc.hpp:188-228):
+ * on every face coded CS_BC_WALL_INVISCID or CS_BC_WALL_VISCOUS, at the face
+ * points with npex == 0 (npex: [lmx] int mask), inviscid: the isentropic total
+ * energy rho^gamma / (gamma (gamma-1)) + |m|^2 / (2 rho); viscous: m = -rho umf
+ * and the isothermal energy rho / (gamma (gamma-1)) + |m|^2 / (2 rho).  The
+ * face plane is index ip * (n - 1) along the axis. */
+int cs_wall_condition_update(double *q, const int *npex, const double umf[3], cs_dcomp d, const int nbc[2][3],
+                             void *stream);
 /* The update physics_base::movef leaves empty (src/physics_base.hpp:147-150):
  * qout = qn - dtk * yaco * de (dtk = dt / (4 - k) for stage k). */
 int cs_rk_update(const double *qn, const double *de, const double *yaco, double dtk, double *qout,

@@ -41,3 +41,17 @@ void gcbc_go(numerics_pc<Type> *numerics_instance, Type *cm_buffer[3], Type *qa,
                                    compact_b200::to_c(dcomp_info), nbc, stream),
                         "gcbc_go");
 }
+
+// wall_condition_update (src/gcbc.hpp:188-228): the wall state at faces coded
+// BC_WALL_INVISCID / BC_WALL_VISCOUS, points where npex == 0.  FP64 and an
+// int mask, as the reference instantiates it.
+template <typename Type, typename TypeIndex>
+void wall_condition_update(Type *qa, TypeIndex *npex, t_point<Type> umf, t_dcomp dcomp_info, int nbc[2][3],
+                           cudaStream_t stream = nullptr) {
+    static_assert(sizeof(Type) == sizeof(double) && sizeof(TypeIndex) == sizeof(int),
+                  "wall_condition_update: double state and int mask");
+    const double u[3] = {umf.x, umf.y, umf.z};
+    compact_b200::check(cs_wall_condition_update(reinterpret_cast<double *>(qa), reinterpret_cast<const int *>(npex),
+                                                 u, compact_b200::to_c(dcomp_info), nbc, stream),
+                        "wall_condition_update");
+}

@@ -276,3 +276,16 @@ class reversed_solves:
 
 def num_threads():
     return lib().or_num_threads()
+
+
+def wall_update(q, npex, dims, nbc, umf=(0.0, 0.0, 0.0)):
+    """In-place wall boundary state update (or_wall_update)."""
+    lxi, let, lze = dims
+    npex = np.ascontiguousarray(npex, dtype=np.int32)
+    nb = (ctypes.c_int * 6)(*[int(nbc[f][a]) for f in range(2) for a in range(3)])
+    u = (ctypes.c_double * 3)(*umf)
+    lib().or_wall_update.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    if lib().or_wall_update(_p(q), npex.ctypes.data_as(ctypes.c_void_p), u, lxi, let, lze, nb):
+        raise ValueError("or_wall_update failed")
+    return q

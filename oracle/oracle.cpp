@@ -801,4 +801,41 @@ void or_tgv_init(double *q, int lxi, int let, int lze, double mach, double amp, 
     }
 }
 
+// Wall boundary state update: wall_condition_update (src/gcbc.hpp:188-228)
+// with wall_inviscid_kernel / wall_viscous_kernel (src/cuda/kernels/gcbc.hpp:160-249).
+// Deviations: the face plane is ip * (n - 1) (the reference's ip * n is one
+// past the end), and the viscous energy uses the updated momentum.
+int or_wall_update(double *q, const int *npex, const double umf[3], int lxi, int let, int lze,
+                   const int nbc[6]) {
+    const int64_t n = (int64_t)lxi * let * lze;
+    const int dims[3] = {lxi, let, lze};
+    const double hamhamm1 = (1.0 / kGam) * kHamm1;
+    for (int a = 0; a < 3; ++a)
+        for (int ip = 0; ip < 2; ++ip) {
+            const int code = nbc[ip * 3 + a];
+            if (code != 20 && code != 25) continue;
+            const int plane = ip * (dims[a] - 1);
+            for (int k = 0; k < lze; ++k)
+                for (int j = 0; j < let; ++j)
+                    for (int i = 0; i < lxi; ++i) {
+                        const int c[3] = {i, j, k};
+                        if (c[a] != plane) continue;
+                        const int64_t idx = i + (int64_t)lxi * (j + (int64_t)let * k);
+                        if (npex[idx] != 0) continue;
+                        const double rho = q[idx];
+                        if (code == 20) {
+                            const double m2 = q[n + idx] * q[n + idx] + q[2 * n + idx] * q[2 * n + idx] +
+                                              q[3 * n + idx] * q[3 * n + idx];
+                            q[4 * n + idx] = hamhamm1 * std::pow(rho, kGam) + 0.5 * m2 / rho;
+                        } else {
+                            for (int d = 0; d < 3; ++d) q[(1 + d) * n + idx] = -rho * umf[d];
+                            const double m2 = q[n + idx] * q[n + idx] + q[2 * n + idx] * q[2 * n + idx] +
+                                              q[3 * n + idx] * q[3 * n + idx];
+                            q[4 * n + idx] = hamhamm1 * rho + 0.5 * m2 / rho;
+                        }
+                    }
+        }
+    return 0;
+}
+
 }  // extern "C"

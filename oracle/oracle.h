@@ -106,6 +106,14 @@ int or_rhs_scaled(const double *q, double *rhs, double mu, or_metrics m, const d
  * (gcbc_go / gcbc_setup_kernel / gcbc_update_non_reflective_kernel,
  * src/gcbc.hpp:86-186, src/cuda/kernels/gcbc.hpp:251-454) with the reference
  * defects fixed.  cm: [2][3][F] face normals, sbcc: [lmx]. */
+/* Wall boundary state update (wall_condition_update, src/gcbc.hpp:188-228;
+ * wall_inviscid_kernel / wall_viscous_kernel, src/cuda/kernels/gcbc.hpp:160-249)
+ * on every face coded BC_WALL_INVISCID (20) or BC_WALL_VISCOUS (25): at the
+ * face's points with npex == 0, inviscid: rho E = rho^gamma / (gamma (gamma-1))
+ * + |m|^2 / (2 rho); viscous: m = -rho umf, rho E = rho / (gamma (gamma-1)) +
+ * |m|^2 / (2 rho) with the updated m.  Face plane ip * (n - 1). */
+int or_wall_update(double *q, const int *npex, const double umf[3], int lxi, int let, int lze,
+                   const int nbc[6]);
 int or_gcbc_x(double *rhs, const double *drva_x, const double *cm, const double *q,
               const double *yaco, const double *sbcc, double c_yaco, const double umf[3],
               int lxi, int let, int lze, const int nbc[2][3]);

@@ -63,6 +63,18 @@ int main() {
     compact_b200::thermo(q, de, p, n);  // restore de[0], de[4] for the fluxes
     phys.calc_fluxes(q, p, de, xim, etm, zem, d, mcd, &pnum, streams);
     compact_b200::rk_update(q, de, yaco, dte / 4.0, q1, n);
+    // wall state at the x faces if they were walls: every point of the mask is
+    // a fluid point (npex = 1), so the state must not change
+    {
+        gcbc<double, int> gc(d);
+        std::vector<int> fluid(n, 1);
+        cudaMemcpy(gc.npex, fluid.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+        int wall[2][3] = {{BC_WALL_VISCOUS, BC_NON_REFLECTIVE, BC_NON_REFLECTIVE},
+                          {BC_WALL_INVISCID, BC_NON_REFLECTIVE, BC_NON_REFLECTIVE}};
+        t_point<double> umf0{0.0, 0.0, 0.0};
+        wall_condition_update(q1, gc.npex, umf0, d, wall);
+        cudaDeviceSynchronize();
+    }
     std::vector<double> r(5 * n);
     cudaMemcpy(r.data(), q1, 5 * n * sizeof(double), cudaMemcpyDeviceToHost);
     double mass = 0;

@@ -150,3 +150,25 @@ def test_dropin_cpp_demo_runs(cuda, tmp_path):
     exe = build_demo(str(tmp_path / "dropin_demo"))
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("nbc", [[[20, 45, 25], [45, 45, 20]], [[25, 20, 45], [20, 25, 25]]])
+def test_wall_condition_update_matches_oracle(cuda, nbc):
+    import torch
+    import compact_schemes_b200 as cs
+    dims = (12, 10, 9)
+    n = int(np.prod(dims))
+    r = np.random.default_rng(3)
+    rho = 1.0 + 0.1 * r.uniform(-1, 1, n)
+    m = 0.1 * r.standard_normal((3, n))
+    E = 1.0 / (1.4 * 0.4) + 0.5 * (m * m).sum(0) / rho
+    q = np.concatenate([rho, m.ravel(), E])
+    npex = (r.uniform(size=n) > 0.4).astype(np.int32)
+    umf = (0.03, -0.01, 0.02)
+    ref = O.wall_update(q.copy(), npex, dims, nbc, umf)
+    qd = torch.from_numpy(q).to(cuda)
+    cs.wall_condition_update(qd, torch.from_numpy(npex).to(cuda), dims, nbc, umf)
+    torch.cuda.synchronize()
+    got = qd.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()
+    assert not np.array_equal(ref, q)  # some wall points changed
