@@ -99,6 +99,8 @@ def declare(L):
         getattr(L, name).restype = i32
     L.cs_solver_autotune.argtypes = [vp, vp, i32, ctypes.POINTER(ctypes.c_int * 3 * 2), vp]
     L.cs_solver_autotune.restype = i32
+    L.cs_vtk_write.argtypes = [ctypes.c_char_p, i32, i32, i32, vp, i32, ctypes.POINTER(ctypes.c_char_p)]
+    L.cs_vtk_write.restype = i32
     L.cs_solver_profile_begin.argtypes = [vp]
     L.cs_solver_profile_end.argtypes = [vp, vp, vp]
     for name in ("cs_solver_create", "cs_solver_destroy", "cs_solver_rhs", "cs_solver_stage",

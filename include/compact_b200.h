@@ -387,6 +387,12 @@ int cs_point_prim(const double q[5], double phi[4]);
 int cs_point_prim_jvp(const double q[5], const double dq[5], double dphi[4]);
 int cs_point_prim_vjp(const double q[5], const double phibar[4], double qbar[5]);
 
+/* Headless VTK output (io::go_vtk, src/IO.hpp:108-159): legacy binary
+ * STRUCTURED_GRID of lxi*let*lze points; data = [nvars][points] host floats,
+ * variables 0..2 the point coordinates, variables 3.. named by names[v-3]. */
+int cs_vtk_write(const char *path, int lxi, int let, int lze, const float *data, int nvars,
+                 const char *const *names);
+
 #ifdef __cplusplus
 }
 #endif
