@@ -41,56 +41,95 @@ __device__ __forceinline__ void deriv_row(int j, int n, int nstart, int nend, do
     else if (j == n - 2) { a = nend ? kAlpha : kAlpha10; c = a; }
 }
 
-// FP32 solve of the derivative of one FP32 line in shared memory with FP64
-// right-hand sides and, if refine, one FP64-residual refinement; the result
-// overwrites the line.
-template <int LT>
-__device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTables<float> &tab, int nstart,
-                                              int nend, const Coeffs &cf, int refine) {
+// FP32 solve of the derivative of G FP32 lines in shared memory (lines[g],
+// g < nf valid) with right-hand sides formed in FP64 and, if refine, one
+// FP64-residual refinement; the results overwrite the lines.  The G fields
+// share each warp_solve (table loads, shuffle latency) and the row
+// coefficients of the residual.
+template <int LT, int G>
+__device__ __forceinline__ void solve_lines_mx(float *const (&lines)[G], int nf, int lane,
+                                               const DevTables<float> &tab, int nstart, int nend,
+                                               const Coeffs &cf, int refine) {
     const int n = tab.n;
     const int len = lane_len(lane, LT, tab.p, tab.last_len);
-    // right-hand side formed in FP64 (its differences cancel), rounded once
-    float r32[LT], x[1][LT];
-    {
-        double r64[LT];
-        deriv_rhs<LT, double, float>(line, n, lane, nstart, nend, nullptr, cf, r64);
+    // right-hand sides formed in FP64 (their differences cancel), rounded once
+    float r32[G][LT], x[G][LT];
 #pragma unroll
-        for (int t = 0; t < LT; ++t) x[0][t] = r32[t] = (float)r64[t];
+    for (int g = 0; g < G; ++g) {
+        if (g < nf) {
+            double r64[LT];
+            deriv_rhs<LT, double, float>(lines[g], n, lane, nstart, nend, nullptr, cf, r64);
+#pragma unroll
+            for (int t = 0; t < LT; ++t) x[g][t] = r32[g][t] = (float)r64[t];
+        } else {
+#pragma unroll
+            for (int t = 0; t < LT; ++t) x[g][t] = r32[g][t] = 0.0f;
+        }
     }
-    warp_solve<LT, 1, float>(tab, x, lane);
+    warp_solve<LT, G, float>(tab, x, lane);
     if (refine) {
-        const float xm0 = __shfl_up_sync(0xffffffffu, x[0][LT - 1], 1);
-        const float xp0 = __shfl_down_sync(0xffffffffu, x[0][0], 1);
-        float e[1][LT];
+        float xm0[G], xp0[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            xm0[g] = __shfl_up_sync(0xffffffffu, x[g][LT - 1], 1);
+            xp0[g] = __shfl_down_sync(0xffffffffu, x[g][0], 1);
+        }
 #pragma unroll
         for (int t = 0; t < LT; ++t) {
             const int j = lane * LT + t;
-            double a, cc;
-            deriv_row(j, n, nstart, nend, a, cc);
-            const double xm = t > 0 ? (double)x[0][t > 0 ? t - 1 : 0] : (double)xm0;
-            double xp = (double)xp0;
+            double ra, rc;
+            deriv_row(j, n, nstart, nend, ra, rc);
 #pragma unroll
-            for (int u = 0; u + 1 < LT; ++u)
-                if (u == t && t + 1 < len) xp = (double)x[0][u + 1];
-            const double res = (double)r32[t] - (a * xm + (double)x[0][t] + cc * xp);
-            e[0][t] = j < n ? (float)res : 0.0f;
+            for (int g = 0; g < G; ++g) {
+                const double xm = t > 0 ? (double)x[g][t > 0 ? t - 1 : 0] : (double)xm0[g];
+                double xp = (double)xp0[g];
+#pragma unroll
+                for (int u = 0; u + 1 < LT; ++u)
+                    if (u == t && t + 1 < len) xp = (double)x[g][u + 1];
+                const double res = (double)r32[g][t] - (ra * xm + (double)x[g][t] + rc * xp);
+                r32[g][t] = j < n ? (float)res : 0.0f;  // the residual replaces the right-hand side
+            }
         }
-        warp_solve<LT, 1, float>(tab, e, lane);
+        warp_solve<LT, G, float>(tab, r32, lane);
 #pragma unroll
-        for (int t = 0; t < LT; ++t) x[0][t] += e[0][t];
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int t = 0; t < LT; ++t) x[g][t] += r32[g][t];
     }
     __syncwarp();
 #pragma unroll
-    for (int t = 0; t < LT; ++t)
-        if (lane * LT + t < n) line[LineLayout<LT>::pos_ct(lane, t)] = x[0][t];
+    for (int g = 0; g < G; ++g) {
+        if (g >= nf) continue;
+#pragma unroll
+        for (int t = 0; t < LT; ++t)
+            if (lane * LT + t < n) lines[g][LineLayout<LT>::pos_ct(lane, t)] = x[g][t];
+    }
 }
 
-// solve_line_mx for the NF fields of this warp's line of the tile.
+template <int LT>
+__device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTables<float> &tab, int nstart,
+                                              int nend, const Coeffs &cf, int refine) {
+    float *const lines[1] = {line};
+    solve_lines_mx<LT, 1>(lines, 1, lane, tab, nstart, nend, cf, refine);
+}
+
+#ifndef CSB_MX_SOLVE_GROUP
+#define CSB_MX_SOLVE_GROUP 2
+#endif
+
+// The NF fields of this warp's line of the tile, CSB_MX_SOLVE_GROUP at a time
+// (one at a time for lines of more than 256 points: registers).
 template <int LT, int TL, int NF>
 __device__ __forceinline__ void solve_fields_mx(float *sm, int w, int lane, const DevTables<float> &tab,
                                                 int nstart, int nend, const Coeffs &cf, int refine) {
+    constexpr int G = LT >= 16 ? 1 : CSB_MX_SOLVE_GROUP;
 #pragma unroll 1
-    for (int c = 0; c < NF; ++c) solve_line_mx<LT>(field_line32<LT, TL>(sm, c, w), lane, tab, nstart, nend, cf, refine);
+    for (int c = 0; c < NF; c += G) {
+        float *lines[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) lines[g] = field_line32<LT, TL>(sm, c + g < NF ? c + g : c, w);
+        solve_lines_mx<LT, G>(lines, NF - c, lane, tab, nstart, nend, cf, refine);
+    }
 }
 
 // FP32 shadow values of one point from the FP64 state (thermo in FP64).
