@@ -336,23 +336,26 @@ def dist_setup(args):
     return world, rank, local
 
 
-def max_over_ranks(x, world):
+def max_over_ranks(x, world, device="cuda"):
+    """Max of a per-rank timing over the process group (the job's time)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
-def barrier(world):
+def barrier(world, cuda=True):
     import torch
-    torch.cuda.synchronize()
+    if cuda:
+        torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    torch.cuda.synchronize()
+    if cuda:
+        torch.cuda.synchronize()
 
 
 def cpu_oracle_stage_rate(n, stages=1):
