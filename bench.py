@@ -21,6 +21,7 @@ weak scaling; the only collective is the timing max).
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -54,6 +55,7 @@ def parse():
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--no-ensemble", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-curvilinear", action="store_true")
     return p.parse_args()
 
 
@@ -104,6 +106,69 @@ def config3_section(args, steps=6):
             "speedup_mixed_vs_plain": out[0]["ms_per_step"] / out[1]["ms_per_step"],
             "rel_err_mixed_vs_fp64_per_field": errs,
             "rel_err_momentum_vs_max_momentum": errs_m, "steps_compared": steps + 1, "unit": UNIT}
+
+
+CURV_STAGE_BYTES = 864 + 3 * 80 + 80 // 4  # + metrics in the 3 flux passes and the dt pass of stage 0
+
+
+def curvilinear_section(args, uniform_ms, steps=20):
+    """The Taylor-Green state on a curvilinear periodic 256^3 grid
+    (x = xi + A sin(eta) sin(zeta) and cyclic, A = 0.1): metrics from
+    cs.grid.metrics, the fused FP64 step reading them per point."""
+    import torch
+    import compact_schemes_b200 as cs
+    n = args.n
+    dims = (n, n, n)
+    lmx = n ** 3
+    h = 2 * math.pi / n
+    ax = torch.arange(n, dtype=torch.float64, device="cuda") * h
+    X, Y, Z = ax.view(1, 1, n), ax.view(1, n, 1), ax.view(n, 1, 1)
+    amp = 0.1
+    xyz = torch.stack([(X + amp * torch.sin(Y) * torch.sin(Z)).expand(n, n, n).reshape(-1),
+                       (Y + amp * torch.sin(Z) * torch.sin(X)).expand(n, n, n).reshape(-1),
+                       (Z + amp * torch.sin(X) * torch.sin(Y)).expand(n, n, n).reshape(-1)]).reshape(-1)
+    nbc = [[cs.BC_PERIODIC] * 3] * 2
+    nm = cs.numerics_pc(dims, nbc)
+    nm.deriv_setup()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    met = cs.grid.metrics(nm, xyz, [[2 * math.pi, 0, 0], [0, 2 * math.pi, 0], [0, 0, 2 * math.pi]])
+    g1.record()
+    torch.cuda.synchronize()
+    metrics_ms = g0.elapsed_time(g1)
+    nm.close()
+    del xyz
+    s = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True))
+    s.set_metrics(*met)
+    q = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
+    cs.tgv_init(q, dims, MACH, 1e-4, 0)
+    choice = s.autotune(q, reps=1)
+    for _ in range(args.warmup):
+        s.step(q)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        s.step(q)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    s.profile_begin()
+    for _ in range(2):
+        s.step(q)
+    prof = s.profile_end()
+    hbm, _ = peaks()
+    stage_ms = sum(v[0] for v in prof.values()) / 8
+    s.close()
+    del met, q
+    torch.cuda.empty_cache()
+    return {"workload": "taylor_green_%d^3 on a curvilinear periodic grid (amplitude 0.1), FP64" % n,
+            "value": lmx * 4 / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "slowdown_vs_uniform": ms / uniform_ms, "grid_metrics_ms": metrics_ms,
+            "schedule": {"%s_%s" % ("grad" if k == 0 else "flux", "xyz"[a]): v for (k, a), v in choice.items()},
+            "passes_ms_per_launch": {k: v[0] / v[1] for k, v in prof.items() if v[1]},
+            "stage_model": {"bytes_per_point": CURV_STAGE_BYTES, "ms_per_stage": stage_ms,
+                            "frac": CURV_STAGE_BYTES * lmx / (stage_ms * 1e-3) / 1e9 / hbm}}
 
 
 def ensemble_section(args):
@@ -543,9 +608,12 @@ def run_ours(args):
                "sample": "1 RK stage of the %d^3 Taylor-Green box in %.1f s (FP64 oracle, "
                          "C++/OpenMP restatement of the reference kernels)" % (n, t)}
 
-    ensemble = adjoint = config3 = None
+    ensemble = adjoint = config3 = curvilinear = None
     if rank == 0 and world == 1:
         s.close()
+        if not args.no_curvilinear:
+            curvilinear = curvilinear_section(args, t_ms / args.steps)
+            torch.cuda.empty_cache()
         if not args.no_mixed:
             config3 = config3_section(args)
             torch.cuda.empty_cache()
@@ -571,6 +639,7 @@ def run_ours(args):
                                         for (k, a), v in tuned.items()}},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed,
                 "config3_mixed_512": config3, "ensemble": ensemble, "adjoint": adjoint,
+                "curvilinear": curvilinear,
                 "gpu_launches": 24 * args.steps, "clocks": clocks,
                 "passes": per_pass,
                 "stage_model": {"bytes_per_point": STAGE_BYTES, "ms_per_stage": stage_ms,

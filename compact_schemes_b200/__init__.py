@@ -91,3 +91,4 @@ from .solver import Solver, SolverConfig, tgv_config, tgv_init  # noqa: E402,F40
 from .physics import physics, physics_rtc, gcbc_go, thermo, rk_update, wall_condition_update  # noqa: E402,F401
 from .ensemble import Ensemble, draw_boxes, ensemble_tgv  # noqa: E402,F401
 from .adjoint import Adjoint  # noqa: E402,F401
+from . import grid  # noqa: E402,F401

@@ -99,6 +99,10 @@ def declare(L):
         getattr(L, name).restype = i32
     L.cs_solver_autotune.argtypes = [vp, vp, i32, ctypes.POINTER(ctypes.c_int * 3 * 2), vp]
     L.cs_solver_autotune.restype = i32
+    L.cs_solver_set_metrics.argtypes = [vp, vp, vp, vp, vp]
+    L.cs_solver_set_metrics.restype = i32
+    L.cs_grid_metrics.argtypes = [vp, vp, ctypes.POINTER(f64 * 3 * 3), vp, vp, vp, vp, vp]
+    L.cs_grid_metrics.restype = i32
     L.cs_vtk_write.argtypes = [ctypes.c_char_p, i32, i32, i32, vp, i32, ctypes.POINTER(ctypes.c_char_p)]
     L.cs_vtk_write.restype = i32
     L.cs_solver_profile_begin.argtypes = [vp]

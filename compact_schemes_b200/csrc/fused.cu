@@ -12,7 +12,9 @@
 //   flux pass a: q, G -> tau, heat flux, flux F[m][a] (m = 0..4) on the fly
 //       -> 5 compact derivatives along a -> R (= for x, += for y) or, for the
 //       last axis, q_out = q^n - dt/(4-k) * J * (R + dF)  (RK update fused).
-// Metrics are those of a uniform Cartesian grid (constants, not read).
+// Metrics are those of a uniform Cartesian grid (constants, not read) unless
+// cs_solver_set_metrics gave per-point arrays; the FP64 one-phase kernels
+// then read them (FM instantiations, 8-line tiles).
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -25,16 +27,26 @@ namespace csb {
 // GCBC, non-reflective, x faces (gcbc_setup_kernel + gcbc_update_non_reflective_kernel,
 // src/cuda/kernels/gcbc.hpp:251-454, reference defects fixed: see oracle/oracle.cpp)
 // ----------------------------------------------------------------------------
+// With per-point metrics (xim_f, yaco_f non-null) the face normal and J are
+// those of the face point and the closure weight is sbcc = 1 / J there.
 template <typename RT>
 __global__ void k_gcbc_x(RT *__restrict__ rhs, const double *__restrict__ drva,
                          const double *__restrict__ q, int lxi, int64_t lmx, int64_t F, int face_mask,
-                         Phys ph, double sb0, double sb1, double sb2, double sb3) {
+                         Phys ph, double sb0, double sb1, double sb2, double sb3,
+                         const double *__restrict__ xim_f = nullptr, const double *__restrict__ yaco_f = nullptr) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 2 * F) return;
     const int ip = (int)(t / F);
     const int64_t fi = t % F;
     if (!((face_mask >> ip) & 1)) return;
     const int64_t idx = fi * lxi + (ip ? lxi - 1 : 0);
+    if (xim_f) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ph.M[0][k] = xim_f[k * lmx + idx];
+        ph.J = yaco_f[idx];
+        sb0 = 1.0 / ph.J;
+        sb1 = sb2 = sb3 = 0.0;
+    }
     // face normal: grad(xi) / |grad(xi)| (exactly (+-1, 0, 0) on a Cartesian grid)
     double c[3];
     if (ph.M[0][1] == 0.0 && ph.M[0][2] == 0.0) {
@@ -127,6 +139,7 @@ struct cs_solver {
     int ndf[2][3]{};
     Coeffs cf{};
     Phys ph{};
+    FieldMet fm{};  // per-point metrics (cs_solver_set_metrics), else null
     TableCache tables;
     const DeviceTables *tab[3] = {nullptr, nullptr, nullptr};
     int active[3] = {0, 0, 0};
@@ -230,6 +243,7 @@ static PassArgs pass_args(cs_solver *s, int a, int kind) {
     p.tab = s->tab[a];
     p.cf = s->cf;
     p.ph = s->ph;
+    p.fm = s->fm;
     p.grad = s->grad;
     p.rhs = s->rhs;
     p.dtacc = s->dtacc;
@@ -318,7 +332,8 @@ static int run_stage(cs_solver *s, const double *qin, const double *qn, double *
                        (s->cfg.nbc[1][0] == CS_BC_NON_REFLECTIVE ? 2 : 0);
             k_gcbc_x<double><<<(unsigned)((2 * F + 127) / 128), 128, 0, st>>>(s->rhs, s->drva, qin, s->d.lxi,
                                                                     s->d.lmx, F, mask, s->ph,
-                                                                    1.0 / s->ph.J, 0.0, 0.0, 0.0);
+                                                                    1.0 / s->ph.J, 0.0, 0.0, 0.0,
+                                                                    s->fm.xim, s->fm.yaco);
             if (cudaGetLastError() != cudaSuccess) { s->rhs = saved_rhs; return set_error(CS_ERR_CUDA, "gcbc launch"); }
         }
     }
@@ -548,8 +563,11 @@ int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3]
         CSB_CUDA(cudaStreamSynchronize(st));
         cs_solver_last_dt(s, &dt);
     }
+    // per-point metrics run the one-phase kernels only
+    const int allowed = s->fm.xim ? 3 : 7;
     for (int c = 0; c < 3 && rc == CS_OK && dt > 0.0; ++c) {
         const int bit = 1 << c;
+        if (!(allowed & bit)) continue;
         for (int k = 0; k < 2; ++k)
             for (int a = 0; a < 3; ++a) {
                 const bool ok = (s->can[k][a] & bit) != 0;
@@ -583,6 +601,25 @@ int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3]
             s->tile[k][a] = pick[k][a] == 0 ? 8 : pick[k][a];
             if (choice) choice[k][a] = pick[k][a];
         }
+    return CS_OK;
+}
+
+int cs_solver_set_metrics(cs_solver *s, const double *xim, const double *etm, const double *zem,
+                          const double *yaco) {
+    if (!s) return set_error(CS_ERR_INVALID, "null argument");
+    const int given = (xim != nullptr) + (etm != nullptr) + (zem != nullptr) + (yaco != nullptr);
+    if (given != 0 && given != 4) return set_error(CS_ERR_INVALID, "give all four metric arrays or none");
+    if (given && s->mixed) return set_error(CS_ERR_UNSUPPORTED, "per-point metrics run in FP64 only");
+    if (given && s->cfg.schedule == CS_SCHED_PIPELINE)
+        return set_error(CS_ERR_UNSUPPORTED, "per-point metrics run the one-phase kernels only");
+    if (given)
+        for (int k = 0; k < 2; ++k)
+            for (int a = 0; a < 3; ++a)
+                if (s->active[a] && s->pl[k][a])
+                    return set_error(CS_ERR_UNSUPPORTED, "axis %d: per-point metrics run the one-phase kernels "
+                                     "only", a);
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
+    s->fm = FieldMet{xim, etm, zem, yaco};
     return CS_OK;
 }
 

@@ -49,6 +49,40 @@ struct Phys {
     double rr1;      // sum of squared metric entries
 };
 
+// Per-point metrics of a curvilinear grid (xim, etm, zem: [3][lmx], yaco:
+// [lmx]; the arrays calc_fluxes_pre_compute_kernel reads,
+// src/cuda/kernels/physics.hpp:42-193).  Kernels compiled with FM = true read
+// them; the others use the constants of Phys.
+struct FieldMet {
+    const double *xim = nullptr, *etm = nullptr, *zem = nullptr, *yaco = nullptr;
+};
+
+// Metric rows and Jacobian at one point.
+struct PointMet {
+    double M[3][3];
+    double J;
+};
+template <bool FM>
+__device__ __forceinline__ PointMet point_met(const Phys &ph, const FieldMet &fm, int64_t lmx, int64_t gi) {
+    PointMet m;
+    if (FM) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            m.M[0][k] = __ldg(fm.xim + k * lmx + gi);
+            m.M[1][k] = __ldg(fm.etm + k * lmx + gi);
+            m.M[2][k] = __ldg(fm.zem + k * lmx + gi);
+        }
+        m.J = __ldg(fm.yaco + gi);
+    } else {
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) m.M[b][k] = ph.M[b][k];
+        m.J = ph.J;
+    }
+    return m;
+}
+
 struct RkParams {
     double div;        // nkrk - k: stage coefficient dt / (nkrk - k)
     double dt_fixed;   // > 0: use it; else CFL dt from dtacc
@@ -123,11 +157,12 @@ __device__ __forceinline__ void solve_fields(double *sm, int w, int lane, const 
 
 // One tile of the gradient pass: lines line0 .. line0+TL-1 (TL * 32 threads;
 // sm holds 4 * TL line slots).
-template <int LT, int AXIS, int TL, bool DTRED>
+template <int LT, int AXIS, int TL, bool DTRED, bool FM = false>
 __device__ __forceinline__ void grad_tile(double *sm, int64_t line0, const double *__restrict__ q,
                                           double *__restrict__ g, const DevTables<double> &tab, int lxi, int let,
                                           int64_t lmx, int64_t F, int nstart, int nend, const Coeffs &cf,
-                                          const Phys &ph, unsigned long long *__restrict__ dtacc) {
+                                          const Phys &ph, unsigned long long *__restrict__ dtacc,
+                                          const FieldMet &fm = FieldMet{}) {
     using L = LineLayout<LT>;
     const int n = tab.n;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -143,13 +178,22 @@ __device__ __forceinline__ void grad_tile(double *sm, int64_t line0, const doubl
         if (DTRED) {
             // calc_time_step_kernel (src/cuda/kernels/physics.hpp:335-427)
             const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
+            const PointMet pm = point_met<FM>(ph, fm, lmx, gi);
+            double rr1 = ph.rr1;
+            if (FM) {
+                rr1 = 0.0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) rr1 += xmul(pm.M[a][c], pm.M[a][c]);
+            }
             double rr2 = 0.0;
 #pragma unroll
             for (int a = 0; a < 3; ++a)
-                rr2 += fabs(xmul(ph.M[a][0], uu) + xmul(ph.M[a][1], vv) + xmul(ph.M[a][2], ww));
-            const double ssi = fabs(ph.J);
-            const double v1 = xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi);
-            const double v2 = s.ri * ph.mu * ph.rr1 * ssi * ssi;
+                rr2 += fabs(xmul(pm.M[a][0], uu) + xmul(pm.M[a][1], vv) + xmul(pm.M[a][2], ww));
+            const double ssi = fabs(pm.J);
+            const double v1 = xmul(sqrt(xmul(s.T, rr1)) + rr2, ssi);
+            const double v2 = s.ri * ph.mu * rr1 * ssi * ssi;
             m1 = fmax(m1, v1);
             m2 = fmax(m2, v2);
         }
@@ -179,14 +223,14 @@ __device__ __forceinline__ void grad_tile(double *sm, int64_t line0, const doubl
 // ----------------------------------------------------------------------------
 // gradient pass: G[AXIS][c] = d/dxi_AXIS of (u, v, w, T)
 // ----------------------------------------------------------------------------
-template <int LT, int AXIS, int TL, bool DTRED>
+template <int LT, int AXIS, int TL, bool DTRED, bool FM = false>
 __global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_GRAD_MINB : 1)
 k_grad(const double *__restrict__ q, double *__restrict__ g, DevTables<double> tab, int lxi, int let,
        int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf, Phys ph,
-       unsigned long long *__restrict__ dtacc) {
+       unsigned long long *__restrict__ dtacc, FieldMet fm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    grad_tile<LT, AXIS, TL, DTRED>(reinterpret_cast<double *>(smem_raw), (int64_t)blockIdx.x * TL, q, g, tab, lxi,
-                                   let, lmx, F, nstart, nend, cf, ph, dtacc);
+    grad_tile<LT, AXIS, TL, DTRED, FM>(reinterpret_cast<double *>(smem_raw), (int64_t)blockIdx.x * TL, q, g, tab,
+                                       lxi, let, lmx, F, nstart, nend, cf, ph, dtacc, fm);
 }
 
 // ----------------------------------------------------------------------------
@@ -199,9 +243,10 @@ enum FluxMode { kWrite = 0, kAccum = 1, kAccumRk = 2, kWriteRk = 3 };
 // with tau / heat flux of calc_viscous_shear_stress_final_kernel, :285-333).
 // CG: the gradients were written earlier in the same launch by other CTAs
 // (ensemble launch) and are read from L2 (ld.global.cg).
-template <int AXIS, bool VISC, bool CG = false>
+template <int AXIS, bool VISC, bool CG = false, bool FM = false>
 __device__ __forceinline__ void point_flux(const double *__restrict__ q, const double *__restrict__ g,
-                                           int64_t lmx, int64_t gi, const Phys &ph, double (&fl)[5]) {
+                                           int64_t lmx, int64_t gi, const Phys &ph, double (&fl)[5],
+                                           const FieldMet &fm = FieldMet{}) {
     const double q0 = __ldg(q + gi), q1 = __ldg(q + lmx + gi), q2 = __ldg(q + 2 * lmx + gi);
     const double q3 = __ldg(q + 3 * lmx + gi), q4 = __ldg(q + 4 * lmx + gi);
     double gr[12];
@@ -210,7 +255,8 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
         for (int k = 0; k < 12; ++k) gr[k] = CG ? __ldcg(g + k * lmx + gi) : __ldg(g + k * lmx + gi);
     }
     const Prim s = primitives(q0, q1, q2, q3, q4);
-    const double *Ma = ph.M[AXIS];
+    const PointMet pm = point_met<FM>(ph, fm, lmx, gi);
+    const double *Ma = pm.M[AXIS];
     const double ss = xmul(Ma[0], s.u + ph.umf[0]) + xmul(Ma[1], s.v + ph.umf[1]) + xmul(Ma[2], s.w + ph.umf[2]);
     fl[0] = xmul(q0, ss);
     fl[1] = xmul(q1, ss) + xmul(Ma[0], s.p);
@@ -225,8 +271,8 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
         for (int c = 0; c < 4; ++c)
 #pragma unroll
             for (int k = 0; k < 3; ++k)
-                dx[c][k] = xmul(ph.M[0][k], gr[c]) + xmul(ph.M[1][k], gr[4 + c]) + xmul(ph.M[2][k], gr[8 + c]);
-        const double muj = xmul(ph.mu, ph.J);
+                dx[c][k] = xmul(pm.M[0][k], gr[c]) + xmul(pm.M[1][k], gr[4 + c]) + xmul(pm.M[2][k], gr[8 + c]);
+        const double muj = xmul(ph.mu, pm.J);
         const double kap = xmul(kGamm1Prndtli, muj);
         const double div = xmul(2.0 / 3.0, dx[0][0] + dx[1][1] + dx[2][2]);
         const double txx = xmul(muj, xmul(2.0, dx[0][0]) - div);
@@ -249,19 +295,21 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
 // CG: the RHS accumulator, gradients and CFL maxima come from other CTAs of
 // the same launch (ensemble) and are read from L2.
 template <int LT, int AXIS, int TL, int MODE, bool VISC, bool CG = false,
-          int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK)>
+          int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK),
+          bool FM = false>
 __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const double *__restrict__ q,
                                           const double *__restrict__ g, double *__restrict__ rhs,
                                           const double *__restrict__ qn, double *__restrict__ qout,
                                           double *__restrict__ drva, const DevTables<double> &tab, int lxi, int let,
                                           int64_t lmx, int64_t F, int nstart, int nend, const Coeffs &cf,
-                                          const Phys &ph, const RkParams &rk) {
+                                          const Phys &ph, const RkParams &rk, const FieldMet &fm = FieldMet{}) {
     using L = LineLayout<LT>;
     const int n = tab.n;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    tile_for_each<AXIS, TL, CSB_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+    // per-point metrics add 10 loads per point: one point per thread in flight
+    tile_for_each<AXIS, TL, FM ? 1 : CSB_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         double fl[5];
-        point_flux<AXIS, VISC, CG>(q, g, lmx, gi, ph, fl);
+        point_flux<AXIS, VISC, CG, FM>(q, g, lmx, gi, ph, fl, fm);
         const int pj = L::pos(j);
 #pragma unroll
         for (int m = 0; m < 5; ++m) field_line<LT, TL>(sm, m, l)[pj] = fl[m];
@@ -281,10 +329,11 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
         }
     }
     tile_sync<AXIS, TL>();
-    double dtk = 0.0;
+    double dtk = 0.0, dtd = 0.0;
     if (MODE >= kAccumRk) {
         const double dt = rk_dt<CG>(rk);
-        dtk = xmul(dt / rk.div, ph.J);
+        dtd = dt / rk.div;
+        dtk = xmul(dtd, ph.J);
         if (rk.dt_out && line0 == 0 && threadIdx.x == 0) *rk.dt_out = dt;
     }
     if (MODE == kWrite) {
@@ -295,10 +344,11 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
         });
     } else {
         // read-modify-write: all loads of a chunk of P points first
-        double rv[P][5], qv[P][5];
+        double rv[P][5], qv[P][5], jv[P];
         tile_for_each_chunked<AXIS, TL, P>(
             line0, F, n, lxi, let,
             [&](int p, int l, int j, int64_t gi) {
+                if (FM && MODE >= kAccumRk) jv[p] = xmul(dtd, __ldg(fm.yaco + gi));
 #pragma unroll
                 for (int m = 0; m < 5; ++m) {
                     rv[p][m] = MODE == kWriteRk ? 0.0 : (CG ? __ldcg(rhs + m * lmx + gi) : rhs[m * lmx + gi]);
@@ -314,22 +364,24 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
                         rhs[m * lmx + gi] = rv[p][m] + dfv;
                     } else {
                         const double r = MODE == kAccumRk ? rv[p][m] + dfv : dfv;
-                        qout[m * lmx + gi] = qv[p][m] - xmul(dtk, r);
+                        qout[m * lmx + gi] = qv[p][m] - xmul(FM ? jv[p] : dtk, r);
                     }
                 }
             });
     }
 }
 
-template <int LT, int AXIS, int TL, int MODE, bool VISC>
+template <int LT, int AXIS, int TL, int MODE, bool VISC, bool FM = false>
 __global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_FLUX_MINB : 1)
 k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__restrict__ rhs,
        const double *__restrict__ qn, double *__restrict__ qout, double *__restrict__ drva,
        DevTables<double> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend,
-       Coeffs cf, Phys ph, RkParams rk) {
+       Coeffs cf, Phys ph, RkParams rk, FieldMet fm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    flux_tile<LT, AXIS, TL, MODE, VISC>(reinterpret_cast<double *>(smem_raw), (int64_t)blockIdx.x * TL, q, g, rhs, qn,
-                                        qout, drva, tab, lxi, let, lmx, F, nstart, nend, cf, ph, rk);
+    constexpr int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK);
+    flux_tile<LT, AXIS, TL, MODE, VISC, false, P, FM>(reinterpret_cast<double *>(smem_raw), (int64_t)blockIdx.x * TL,
+                                                      q, g, rhs, qn, qout, drva, tab, lxi, let, lmx, F, nstart, nend,
+                                                      cf, ph, rk, fm);
 }
 
 
@@ -351,6 +403,7 @@ struct PassArgs {
     const DeviceTables *tab;
     Coeffs cf;
     Phys ph;
+    FieldMet fm;   // per-point metrics (xim null: the constants of ph)
     double *grad;  // [3][4][lmx]
     double *rhs;   // [5][lmx]
     unsigned long long *dtacc;
@@ -378,10 +431,11 @@ template <int LT, int AXIS, int TL>
 int launch_grad_t(const PassArgs &a, const double *q, bool dtred, cudaStream_t st) {
     const size_t smem = (size_t)4 * TL * LineLayout<LT>::kSlot * sizeof(double);
     auto kern = dtred ? k_grad<LT, AXIS, TL, true> : k_grad<LT, AXIS, TL, false>;
+    if (dtred && a.fm.xim) kern = k_grad<LT, AXIS, TL, true, true>;
     if (int rc = set_smem(kern, smem)) return rc;
     const unsigned blocks = (unsigned)((a.F + TL - 1) / TL);
     kern<<<blocks, TL * 32, smem, st>>>(q, a.grad + (int64_t)AXIS * 4 * a.lmx, a.tab->t64, a.lxi, a.let,
-                                        a.lmx, a.F, a.nstart, a.nend, a.cf, a.ph, a.dtacc);
+                                        a.lmx, a.F, a.nstart, a.nend, a.cf, a.ph, a.dtacc, a.fm);
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }
@@ -391,10 +445,11 @@ int launch_flux_t(const PassArgs &a, const double *q, const double *qn, double *
                   const RkParams &rk, cudaStream_t st) {
     const size_t smem = (size_t)5 * TL * LineLayout<LT>::kSlot * sizeof(double);
     auto kern = a.viscous ? k_flux<LT, AXIS, TL, MODE, true> : k_flux<LT, AXIS, TL, MODE, false>;
+    if (a.fm.xim) kern = a.viscous ? k_flux<LT, AXIS, TL, MODE, true, true> : k_flux<LT, AXIS, TL, MODE, false, true>;
     if (int rc = set_smem(kern, smem)) return rc;
     const unsigned blocks = (unsigned)((a.F + TL - 1) / TL);
     kern<<<blocks, TL * 32, smem, st>>>(q, a.grad, a.rhs, qn, qout, drva, a.tab->t64, a.lxi, a.let, a.lmx,
-                                        a.F, a.nstart, a.nend, a.cf, a.ph, rk);
+                                        a.F, a.nstart, a.nend, a.cf, a.ph, rk, a.fm);
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }

@@ -113,6 +113,14 @@ class Solver:
         check(lib().cs_solver_autotune(self._h, ptr(q), int(reps), ctypes.byref(ch), stream_ptr(stream)))
         return {(k, a): ch[k][a] for k in range(2) for a in range(3)}
 
+    def set_metrics(self, xim=None, etm=None, zem=None, yaco=None):
+        """Per-point metrics (torch CUDA float64: xim/etm/zem [3*lmx], yaco
+        [lmx]) for every later call; no arguments returns to the uniform grid.
+        The tensors are kept alive by the solver."""
+        arrs = (xim, etm, zem, yaco)
+        check(lib().cs_solver_set_metrics(self._h, *(None if a is None else ptr(a) for a in arrs)))
+        self._metrics = arrs if xim is not None else None
+
     def last_dt(self):
         v = ctypes.c_double()
         check(lib().cs_solver_last_dt(self._h, ctypes.byref(v)))

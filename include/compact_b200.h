@@ -179,6 +179,22 @@ int cs_calc_time_step(cs_physics *ph, const double *xim, const double *etm, cons
  * (driver/canard.cu:142-143): de0 = 1/rho, de1..3 = u, v, w,
  * de4 = gamma p / rho (T in CANARD units, rho_inf = c_inf = 1), p. */
 int cs_thermo(const double *q, double *de, double *p, size_t n, void *stream);
+/* Metrics and Jacobian of a curvilinear grid, the arrays the flux kernels
+ * read (xim, etm, zem = J^-1 grad(xi_a), yaco = J;
+ * src/cuda/kernels/physics.hpp:42-193), which the reference's grid class does
+ * not generate (grid::generate, src/grid.hpp:89-213, makes coordinates only).
+ * Cross-product form with the compact derivative of nm (its closures):
+ * xim = r_eta x r_zeta, etm = r_zeta x r_xi, zem = r_xi x r_eta,
+ * yaco = 1 / (r_xi . xim).  xyz: [3][lmx] device coordinates; period[a][c]
+ * (nullable): the jump of coordinate c across axis a, used on axes whose ndf
+ * is 1 (r_a = D(c - i_a period/n_a) + period/n_a).  Outputs are device
+ * arrays [3][lmx] (xim, etm, zem) and [lmx] (yaco).  Needs cs_deriv_setup;
+ * overwrites nm's drva variable 0; allocates 10 lmx doubles for the call
+ * (stream-ordered) and synchronizes the stream.  CS_ERR_INVALID on a cell of
+ * zero volume. */
+int cs_grid_metrics(cs_numerics *nm, const double *xyz, const double period[3][3], double *xim,
+                    double *etm, double *zem, double *yaco, void *stream);
+
 /* Wall boundary state update, wall_condition_update (src/gcbc.hpp:188-228):
  * on every face coded CS_BC_WALL_INVISCID or CS_BC_WALL_VISCOUS, at the face
  * points with npex == 0 (npex: [lmx] int mask), inviscid: the isentropic total
@@ -276,6 +292,16 @@ int cs_solver_dt_device(cs_solver *s, double **dt_dev);
  * receives 8 or 16 (one-phase tile lines) or 0 (pipelined) for the gradient
  * (kind 0) and flux (kind 1) passes.  Synchronizes. */
 int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3], void *stream);
+/* Per-point metrics for the fused solver: device arrays xim, etm, zem
+ * ([3][lmx], J^-1 grad(xi_a)) and yaco ([lmx], J), as cs_grid_metrics
+ * writes them, read by every later step, stage and RHS call instead of the
+ * uniform grid of dx, dy, dz (the arrays must outlive that use; all four null
+ * returns to the uniform grid).  FP64 only; the passes run the one-phase
+ * kernels (CS_ERR_UNSUPPORTED for CS_PREC_MIXED or pipelined passes; the
+ * autotuner then picks among the one-phase tiles).  With GCBC the face normal
+ * and J are those of each face point. */
+int cs_solver_set_metrics(cs_solver *s, const double *xim, const double *etm, const double *zem,
+                          const double *yaco);
 int cs_solver_profile_begin(cs_solver *s);
 int cs_solver_profile_end(cs_solver *s, double ms[CS_PASS_KINDS], int launches[CS_PASS_KINDS]);
 /* Taylor-Green initial state on a periodic [0,2pi)^3 grid in CANARD units

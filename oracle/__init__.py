@@ -70,6 +70,8 @@ def lib():
         L.or_rk_step.restype = f64
         L.or_rk_stage.argtypes = [vp, vp, vp, i32, f64, f64, Metrics, vp, i32, i32, i32, vp, i32]
         L.or_rk_stage.restype = f64
+        L.or_grid_metrics.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp, vp, vp]
+        L.or_grid_metrics.restype = i32
         L.or_tgv_init.argtypes = [vp, i32, i32, i32, f64, f64, ctypes.c_uint64]
         L.or_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.or_noise.restype = f64
@@ -251,6 +253,22 @@ def rk_stage(qn, qin, qout, k, dt, mu, metrics, dims, nbc, viscous=True, umf=(0.
                           int(viscous))
     if r < 0:
         raise ValueError("or_rk_stage failed")
+
+
+def grid_metrics(xyz, dims, nbc, period=None):
+    """Metrics of the grid with coordinates xyz ([3][lmx]); returns a Metrics
+    with per-point arrays (xim, etm, zem: [3][lmx], yaco: [lmx])."""
+    lxi, let, lze = dims
+    n = lxi * let * lze
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+    per = np.zeros((3, 3)) if period is None else np.ascontiguousarray(period, dtype=np.float64)
+    ndf = (np.asarray(nbc) >= BC_INTER_STRAIGHT).astype(np.int32)
+    nd, ndp = _ip(ndf)
+    xim, etm, zem, yaco = np.empty(3 * n), np.empty(3 * n), np.empty(3 * n), np.empty(n)
+    rc = lib().or_grid_metrics(_p(xyz), _p(per), lxi, let, lze, ndp, _p(xim), _p(etm), _p(zem), _p(yaco))
+    if rc:
+        raise ValueError("or_grid_metrics failed (%d)" % rc)
+    return field_metrics(xim, etm, zem, yaco)
 
 
 def tgv_init(dims, mach=0.1, noise=1e-4, seed=0):

@@ -725,6 +725,18 @@ double or_rk_step(double *q, double mu, or_metrics m, const double umf[3], int l
         drva.assign(10 * F, 0.0);
         cm.assign(6 * F, 0.0);
         for (int64_t i = 0; i < F; ++i) { cm[i] = 1.0; cm[3 * F + i] = 1.0; }
+        if (m.xim) {
+            // curvilinear: the face normal is grad(xi) / |grad(xi)| at the face point
+            for (int ip = 0; ip < 2; ++ip)
+                for (int64_t fi = 0; fi < F; ++fi) {
+                    const int64_t idx = fi * lxi + (ip ? lxi - 1 : 0);
+                    const double x0 = m.xim[idx], x1 = m.xim[n + idx], x2 = m.xim[2 * n + idx];
+                    const double nrm = std::sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+                    cm[(ip * 3 + 0) * F + fi] = x0 / nrm;
+                    cm[(ip * 3 + 1) * F + fi] = x1 / nrm;
+                    cm[(ip * 3 + 2) * F + fi] = x2 / nrm;
+                }
+        }
         sbcc.assign(n, 0.0);
         for (int64_t fi = 0; fi < F; ++fi) {
             int64_t i0 = fi * lxi, i1 = fi * lxi + lxi - 1;
@@ -767,6 +779,60 @@ double or_rk_stage(const double *qn, const double *qin, double *qout, int k, dou
         for (int v = 0; v < 5; ++v) qout[v * n + i] = qn[v * n + i] - dtk * J * rhs[v * n + i];
     }
     return dt;
+}
+
+// Metrics and Jacobian of a curvilinear grid.  The reference's grid class only
+// generates coordinates (grid::generate, src/grid.hpp:89-213); the metric
+// arrays its physics kernels read (xim, etm, zem = J^-1 grad xi_a, yaco = J,
+// src/cuda/kernels/physics.hpp:42-193) have no generator there.  This is the
+// cross-product form with index-space compact derivatives r_a = d r / d xi_a:
+//   xim = r_eta x r_zeta,  etm = r_zeta x r_xi,  zem = r_xi x r_eta,
+//   yaco = 1 / (r_xi . xim).
+// On an axis with interface closures the coordinate c is split into a
+// periodic part and a ramp, c = c~ + i_a * s, s = period[a][c] / n_a, and
+// r_a = D c~ + s.
+int or_grid_metrics(const double *xyz, const double period[3][3], int lxi, int let, int lze,
+                    const int ndf[2][3], double *xim, double *etm, double *zem, double *yaco) {
+    ensure_coeffs();
+    const int64_t n = (int64_t)lxi * let * lze;
+    const int dims[3] = {lxi, let, lze};
+    std::vector<double> d(9 * n), tmp(n);
+    for (int a = 0; a < 3; ++a) {
+        const bool ramp = ndf[0][a] || ndf[1][a];
+        for (int c = 0; c < 3; ++c) {
+            const double sl = ramp ? period[a][c] / dims[a] : 0.0;
+            const double *src = xyz + c * n;
+#pragma omp parallel for
+            for (int64_t i = 0; i < n; ++i) {
+                const int64_t ia = a == 0 ? i % lxi : (a == 1 ? (i / lxi) % let : i / ((int64_t)lxi * let));
+                tmp[i] = src[i] - (double)ia * sl;
+            }
+            double *dc = d.data() + (a * 3 + c) * n;
+            int rc = or_deriv(tmp.data(), dc, lxi, let, lze, a, ndf[0][a], ndf[1][a], nullptr, nullptr, 0,
+                              g_pbco, g_pbci);
+            if (rc) return rc;
+#pragma omp parallel for
+            for (int64_t i = 0; i < n; ++i) dc[i] += sl;
+        }
+    }
+    int err = 0;
+#pragma omp parallel for reduction(|: err)
+    for (int64_t i = 0; i < n; ++i) {
+        double r[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 3; ++c) r[a][c] = d[(a * 3 + c) * n + i];
+        double *out[3] = {xim, etm, zem};
+        for (int a = 0; a < 3; ++a) {
+            const double *p = r[(a + 1) % 3], *q = r[(a + 2) % 3];
+            out[a][i] = p[1] * q[2] - p[2] * q[1];
+            out[a][n + i] = p[2] * q[0] - p[0] * q[2];
+            out[a][2 * n + i] = p[0] * q[1] - p[1] * q[0];
+        }
+        const double vol = r[0][0] * xim[i] + r[0][1] * xim[n + i] + r[0][2] * xim[2 * n + i];
+        if (!(vol != 0.0)) err = 1;
+        yaco[i] = 1.0 / vol;
+    }
+    return err ? -2 : 0;
 }
 
 // splitmix64 of (seed, index) mapped to [-1, 1): a counter-based generator

@@ -130,6 +130,13 @@ double or_rk_stage(const double *qn, const double *qin, double *qout, int k, dou
                    or_metrics m, const double umf[3], int lxi, int let, int lze, const int nbc[2][3],
                    int viscous);
 
+/* Metrics (xim, etm, zem: [3][n]) and Jacobian (yaco: [n]) of the grid with
+ * coordinates xyz ([3][n]), cross-product form with compact derivatives;
+ * period[a][c]: jump of coordinate c across axis a (axes with ndf = 1).
+ * Returns 0, -1 on a bad size, -2 on a zero cell volume. */
+int or_grid_metrics(const double *xyz, const double period[3][3], int lxi, int let, int lze,
+                    const int ndf[2][3], double *xim, double *etm, double *zem, double *yaco);
+
 /* Taylor-Green initial state on a periodic [0,2pi)^3 grid (CANARD units:
  * rho0 = 1, c_inf = 1, p0 = 1/gamma), density noise amp*U(-1,1) from the
  * counter-based generator or_noise. */
