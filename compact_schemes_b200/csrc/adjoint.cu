@@ -40,6 +40,9 @@ struct cs_adjoint {
     // terms at the faces [2][5][F], face adjoint of q, lambda for the x solve [5][lmx]
     int gcbc_mask = 0;
     double *rf = nullptr, *drf = nullptr, *qbf = nullptr, *lamx = nullptr;
+    // sweep buffer of cs_adjoint_gradient, kept for the next call
+    double *sweep = nullptr;
+    size_t sweep_bytes = 0;
 };
 
 namespace csb {
@@ -247,7 +250,7 @@ int cs_adjoint_destroy(cs_adjoint *a) {
     if (!a) return set_error(CS_ERR_INVALID, "null argument");
     if (a->fwd) cs_solver_destroy(a->fwd);
     for (double *p : {a->G, a->G2, a->phi4, a->F15, a->qbar, a->t1, a->t2, a->t3, a->partial, a->rf, a->drf, a->qbf,
-                      a->lamx})
+                      a->lamx, a->sweep})
         cudaFree(p);
     cudaFree(a->dtacc);
     delete a;
@@ -419,12 +422,23 @@ int cs_adjoint_gradient(cs_adjoint *a, const double *q0, int nsteps, const doubl
     const int nseg = (nsteps + every - 1) / every;
     const int segmax = every < nsteps ? every : nsteps;
     // checkpoints, the running state, the stage states of one segment, two adjoint states
-    double *buf = nullptr;
     const int64_t nbuf = (int64_t)nseg + 1 + 4LL * segmax + 2;
-    if (cudaMalloc(&buf, nbuf * bytes) != cudaSuccess) return set_error(CS_ERR_ALLOC, "adjoint checkpoint allocation");
+    if (a->sweep_bytes < (size_t)nbuf * bytes) {
+        // a larger sweep than any before: replace the kept buffer (a 4 GB
+        // allocation costs far more than a reverse step, so it is reused)
+        if (a->sweep) cudaFree(a->sweep);
+        a->sweep = nullptr;
+        a->sweep_bytes = 0;
+        if (cudaMalloc(&a->sweep, nbuf * bytes) != cudaSuccess) {
+            a->sweep = nullptr;
+            return set_error(CS_ERR_ALLOC, "adjoint checkpoint allocation");
+        }
+        a->sweep_bytes = (size_t)nbuf * bytes;
+    }
+    double *buf = a->sweep;
     double *ckpt = buf, *qrun = buf + nseg * n5, *seg = qrun + n5, *lamA = seg + 4LL * segmax * n5, *lamB = lamA + n5;
     int rc = CS_OK;
-    auto fail = [&](int r) { cudaFree(buf); return r; };
+    auto fail = [&](int r) { return r; };
     // forward sweep: checkpoint every `every` steps
     if (cudaMemcpyAsync(qrun, q0, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return fail(set_error(CS_ERR_CUDA, "state copy"));
@@ -462,7 +476,6 @@ int cs_adjoint_gradient(cs_adjoint *a, const double *q0, int nsteps, const doubl
         return fail(set_error(CS_ERR_CUDA, "gradient copy"));
     if (cudaStreamSynchronize(st) != cudaSuccess) return fail(set_error(CS_ERR_CUDA, "adjoint sweep"));
     if (J_host) *J_host = J;
-    cudaFree(buf);
     return CS_OK;
 }
 

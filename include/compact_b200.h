@@ -394,7 +394,9 @@ int cs_kinetic_energy(cs_adjoint *a, const double *q, double *J_host, double *dJ
 /* dJ/dq0 of J = kinetic energy after nsteps steps with time steps dt_host[s]:
  * forward sweep keeping a checkpoint every `every` steps, then a reverse sweep
  * that recomputes each segment's stage states from its checkpoint and applies
- * cs_step_vjp step by step.  Synchronizes. */
+ * cs_step_vjp step by step.  Synchronizes.  The sweep buffer
+ * (cs_adjoint_gradient_bytes) stays allocated for later calls until
+ * cs_adjoint_destroy. */
 int cs_adjoint_gradient(cs_adjoint *a, const double *q0, int nsteps, const double *dt_host, int every,
                         double *grad_q0, double *J_host, void *stream);
 /* Device bytes cs_adjoint_gradient allocates for its sweeps (checkpoints,
