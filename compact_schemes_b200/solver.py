@@ -134,8 +134,10 @@ def tgv_init(q, dims, mach=0.1, noise=1e-4, seed=0, stream=None):
 
 
 def _main(argv=None):
-    """python -m compact_schemes_b200.solver --n N [--precision P] [--steps K]:
-    K CFL-stepped RK steps of the N^3 Taylor-Green box (profiling driver)."""
+    """python -m compact_schemes_b200.solver --n N [--precision P] [--steps K] [--curvilinear A]:
+    K CFL-stepped RK steps of the N^3 Taylor-Green box (profiling driver);
+    with A > 0 on the periodic wavy grid x = xi + A sin(eta) sin(zeta)
+    (and cyclic), metrics read per point."""
     import argparse
     import torch
     p = argparse.ArgumentParser()
@@ -143,9 +145,23 @@ def _main(argv=None):
     p.add_argument("--precision", type=int, default=PREC_FP64)
     p.add_argument("--steps", type=int, default=1)
     p.add_argument("--graph", type=int, default=0)
+    p.add_argument("--curvilinear", type=float, default=0.0)
     a = p.parse_args(argv)
     from compact_schemes_b200 import solver as S  # the package's classes, not __main__'s
     s = S.Solver(S.tgv_config(a.n, precision=a.precision, use_graph=bool(a.graph)))
+    if a.curvilinear > 0:
+        import compact_schemes_b200 as cs
+        n = a.n
+        ax = torch.arange(n, dtype=torch.float64, device="cuda") * (2 * math.pi / n)
+        X, Y, Z = ax.view(1, 1, n), ax.view(1, n, 1), ax.view(n, 1, 1)
+        A = a.curvilinear
+        xyz = torch.stack([(X + A * torch.sin(Y) * torch.sin(Z)).expand(n, n, n).reshape(-1),
+                           (Y + A * torch.sin(Z) * torch.sin(X)).expand(n, n, n).reshape(-1),
+                           (Z + A * torch.sin(X) * torch.sin(Y)).expand(n, n, n).reshape(-1)]).reshape(-1)
+        nm = cs.numerics_pc((n, n, n), [[BC_PERIODIC] * 3] * 2)
+        nm.deriv_setup()
+        s.set_metrics(*cs.grid.metrics(nm, xyz, [[2 * math.pi, 0, 0], [0, 2 * math.pi, 0], [0, 0, 2 * math.pi]]))
+        nm.close()
     q = torch.empty(5 * a.n ** 3, dtype=torch.float64, device="cuda")
     S.tgv_init(q, (a.n, a.n, a.n))
     for _ in range(a.steps):
