@@ -92,3 +92,4 @@ from .physics import physics, physics_rtc, gcbc_go, thermo, rk_update, wall_cond
 from .ensemble import Ensemble, draw_boxes, ensemble_tgv  # noqa: E402,F401
 from .adjoint import Adjoint  # noqa: E402,F401
 from . import grid  # noqa: E402,F401
+from .domdcomp import domdcomp, mpigo as mpigo_dist, mpigo_local  # noqa: E402,F401
