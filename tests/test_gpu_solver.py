@@ -229,3 +229,23 @@ def test_headline_rhs_256(cuda):
     floor = rhs_err(ref2, ref, scale)
     err = rhs_err(got, ref, scale)
     assert err <= max(1e-12, 2.0 * floor), (err, floor)
+
+
+@pytest.mark.parametrize("dims,gcbc", [((37, 29, 23), False), ((45, 19, 27), True)])
+def test_odd_sizes_rk_steps_match_oracle(cuda, dims, gcbc):
+    """Ragged lines: lengths that fill neither a warp's lanes nor their chunks."""
+    import torch
+    nbc = [[10, 45, 45], [10, 45, 45]] if gcbc else [[45] * 3, [45] * 3]
+    s = solver(dims, use_graph=False, nbc=nbc, gcbc=gcbc)
+    q = O.tgv_init(dims, 0.3 if gcbc else MACH, 1e-4, 2)
+    qd = dev(q)
+    qr = q.copy()
+    dt = None
+    for _ in range(3):
+        s.step(qd, 0.0)
+        dt = O.rk_step(qr, MU, O.uniform_metrics(*dims), dims, nbc, cfl=0.5, gcbc=gcbc)
+    torch.cuda.synchronize()
+    assert abs(s.last_dt() - dt) / dt < 1e-13
+    got = qd.cpu().numpy().reshape(5, -1)
+    ref = qr.reshape(5, -1)
+    assert max(np.abs(got[m] - ref[m]).max() / np.abs(ref[m]).max() for m in (0, 1, 2, 4)) < 1e-12
