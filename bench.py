@@ -597,7 +597,7 @@ def run_ours(args):
                  "rel_err_vs_fp64_per_field": dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_E"], errs)),
                  "rel_err_momentum_vs_max_momentum": errs_m,
                  "steps_compared": args.steps + args.warmup,
-                 "arith": "FP32 fluxes/line solves; FP64 state, RK, thermo, RHS rows, refinement residual"}
+                 "arith": "FP32 fluxes/line solves; FP64 state, RK, thermo, RHS rows; no refinement sweep"}
         sm.close()
         del qm, qp
 

@@ -273,7 +273,9 @@ static MixedArgs mixed_args(cs_solver *s, int a, int kind) {
     m.shadow = s->sh32;
     m.grad = s->grad32;
     m.rhs = s->rhs32;
-    m.refine = s->cfg.refine;
+    // CS_REFINE_FLUX: the gradient passes skip the refinement sweep (their
+    // FP32 solve error only reaches the state through the viscous terms)
+    m.refine = s->cfg.refine == CS_REFINE_FLUX ? (kind == 1) : s->cfg.refine;
     return m;
 }
 
@@ -433,6 +435,10 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
     if (cfg->precision != CS_PREC_FP64 && cfg->precision != CS_PREC_MIXED) {
         delete s;
         return set_error(CS_ERR_INVALID, "precision %d", cfg->precision);
+    }
+    if (cfg->refine < CS_REFINE_NONE || cfg->refine > CS_REFINE_FLUX) {
+        delete s;
+        return set_error(CS_ERR_INVALID, "refine %d", cfg->refine);
     }
     if (cfg->schedule < CS_SCHED_AUTO || cfg->schedule > CS_SCHED_PIPELINE) {
         delete s;

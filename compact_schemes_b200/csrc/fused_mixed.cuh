@@ -14,8 +14,11 @@
 //     RHS unchanged while the FP32 derivative of a pressure-dominated flux
 //     keeps its precision;
 //   * line solves in FP32 on right-hand sides formed in FP64 (closure rows
-//     included), followed by one iterative-refinement sweep whose residual
-//     r - A x is formed in FP64.
+//     included), optionally followed by one iterative-refinement sweep whose
+//     residual r - A x is formed in FP64 (cfg.refine: none, all passes, or
+//     the flux passes only).  The state error against the FP64 path is set by
+//     the FP32 shadow, gradients and RHS accumulator, not by the solves: it is
+//     the same with and without the sweep.
 #pragma once
 
 #include "fused_kernels.cuh"

@@ -24,13 +24,16 @@ class SolverConfig(ctypes.Structure):
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+REFINE_NONE = 0  # mixed: no refinement sweep (the measured state error is the same)
+REFINE_ALL = 1   # mixed: a refinement sweep after every FP32 line solve
+REFINE_FLUX = 2  # mixed: refinement in the flux passes only
 SCHED_AUTO = 0
 SCHED_ONEPHASE = 1
 SCHED_PIPELINE = 2
 
 
 def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, dims=None,
-               nbc=None, gcbc=False, tile=None, precision=PREC_FP64, refine=1, schedule=SCHED_AUTO):
+               nbc=None, gcbc=False, tile=None, precision=PREC_FP64, refine=REFINE_NONE, schedule=SCHED_AUTO):
     """Taylor-Green box [0,2pi)^3 in CANARD units: mu = rho0 U0 L / Re with U0 = Mach."""
     lxi, let, lze = dims if dims is not None else (n, n, n)
     c = SolverConfig()

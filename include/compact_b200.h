@@ -232,9 +232,13 @@ int cs_gcbc_go(cs_numerics *nm, double *const cm[3], const double *qa, double *d
 typedef struct cs_solver cs_solver;
 
 #define CS_PREC_FP64 0  /* plain FP64 */
-#define CS_PREC_MIXED 1 /* FP32 fluxes and line solves (FP64 right-hand sides and one
-                           FP64-residual refinement sweep), FP64 state, RK accumulation
-                           and thermodynamics */
+#define CS_PREC_MIXED 1 /* FP32 fluxes and line solves (FP64 right-hand sides, refinement
+                           as cfg.refine), FP64 state, RK accumulation and thermodynamics */
+
+#define CS_REFINE_NONE 0 /* mixed: no refinement sweep */
+#define CS_REFINE_ALL 1  /* mixed: a refinement sweep after every FP32 line solve */
+#define CS_REFINE_FLUX 2 /* mixed: refinement in the flux passes only; the gradients feed the
+                            state only through the viscous terms */
 
 #define CS_SCHED_AUTO 0     /* the measured-faster schedule: one-phase on B200 */
 #define CS_SCHED_ONEPHASE 1 /* each CTA loads a tile, solves it, stores it (tile[][] applies) */
@@ -256,7 +260,8 @@ typedef struct {
                            tiles that do not fit shared memory fall back to 8; the mixed
                            form uses 8 for y */
     int precision;      /* CS_PREC_FP64 or CS_PREC_MIXED */
-    int refine;         /* mixed: one FP64-residual refinement sweep per line solve (1) or none (0) */
+    int refine;         /* mixed: CS_REFINE_ALL one FP64-residual refinement sweep per line
+                           solve, CS_REFINE_NONE none, CS_REFINE_FLUX in the flux passes only */
     int schedule;       /* CS_SCHED_*: how a pass overlaps its line solves with its HBM traffic */
 } cs_solver_config;
 

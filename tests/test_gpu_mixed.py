@@ -1,5 +1,5 @@
-"""Mixed-precision form: FP32 fluxes and line solves (FP64 right-hand sides and
-one FP64-residual refinement sweep), FP64 state, RK accumulation and
+"""Mixed-precision form: FP32 fluxes and line solves (FP64 right-hand sides,
+an optional FP64-residual refinement sweep), FP64 state, RK accumulation and
 thermodynamics.
 
 Target (north star): relative state error <= 1e-6 per field after 100 RK steps
@@ -27,7 +27,7 @@ def make(dims, precision, **kw):
     return cs.Solver(cs.tgv_config(None, dims=dims, precision=precision, **kw))
 
 
-@pytest.mark.parametrize("refine", [1, 0])
+@pytest.mark.parametrize("refine", [1, 0, 2])
 def test_mixed_rhs_vs_oracle(cuda, refine):
     """Mixed RHS against the FP64 oracle, relative to the size of the summed terms."""
     import torch
@@ -43,7 +43,8 @@ def test_mixed_rhs_vs_oracle(cuda, refine):
     assert err < 2e-6, err
 
 
-def test_mixed_100_steps_within_1e6(cuda):
+@pytest.mark.parametrize("refine", [0, 1, 2])
+def test_mixed_100_steps_within_1e6(cuda, refine):
     import torch
     import compact_schemes_b200 as cs
     dims = (64, 64, 64)
@@ -51,13 +52,13 @@ def test_mixed_100_steps_within_1e6(cuda):
     q0 = torch.empty(5 * n, dtype=torch.float64, device="cuda")
     cs.tgv_init(q0, dims, MACH, 1e-4, 0)
     qp, qm = q0.clone(), q0.clone()
-    sp, sm = make(dims, 0), make(dims, 1)
+    sp, sm = make(dims, 0), make(dims, 1, refine=refine)
     for _ in range(100):
         sp.step(qp, 0.0)
         sm.step(qm, 0.0)
     torch.cuda.synchronize()
     errs = per_field(qm, qp, n)
-    print("mixed vs FP64 after 100 steps at 64^3, per field:", errs)
+    print("mixed (refine %d) vs FP64 after 100 steps at 64^3, per field:" % refine, errs)
     assert max(errs[:3] + errs[4:]) <= 1e-6, errs
     assert errs[3] <= 1e-5, errs
 
