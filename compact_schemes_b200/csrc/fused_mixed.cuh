@@ -21,6 +21,8 @@
 //     the same with and without the sweep.
 #pragma once
 
+#include <type_traits>
+
 #include "fused_kernels.cuh"
 
 namespace csb {
@@ -48,8 +50,9 @@ __device__ __forceinline__ void deriv_row(int j, int n, int nstart, int nend, do
 // g < nf valid) with right-hand sides formed in FP64 and, if refine, one
 // FP64-residual refinement; the results overwrite the lines.  The G fields
 // share each warp_solve (table loads, shuffle latency) and the row
-// coefficients of the residual.
-template <int LT, int G>
+// coefficients of the residual.  MAYREF = false compiles the sweep out (the
+// kernels without refinement then need fewer registers).
+template <int LT, int G, bool MAYREF = true>
 __device__ __forceinline__ void solve_lines_mx(float *const (&lines)[G], int nf, int lane,
                                                const DevTables<float> &tab, int nstart, int nend,
                                                const Coeffs &cf, int refine) {
@@ -70,7 +73,7 @@ __device__ __forceinline__ void solve_lines_mx(float *const (&lines)[G], int nf,
         }
     }
     warp_solve<LT, G, float>(tab, x, lane);
-    if (refine) {
+    if (MAYREF && refine) {
         float xm0[G], xp0[G];
 #pragma unroll
         for (int g = 0; g < G; ++g) {
@@ -122,16 +125,16 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
 
 // The NF fields of this warp's line of the tile, CSB_MX_SOLVE_GROUP at a time
 // (one at a time for lines of more than 256 points: registers).
-template <int LT, int TL, int NF>
+template <int LT, int TL, int NF, bool REF>
 __device__ __forceinline__ void solve_fields_mx(float *sm, int w, int lane, const DevTables<float> &tab,
-                                                int nstart, int nend, const Coeffs &cf, int refine) {
+                                                int nstart, int nend, const Coeffs &cf) {
     constexpr int G = LT >= 16 ? 1 : CSB_MX_SOLVE_GROUP;
 #pragma unroll 1
     for (int c = 0; c < NF; c += G) {
         float *lines[G];
 #pragma unroll
         for (int g = 0; g < G; ++g) lines[g] = field_line32<LT, TL>(sm, c + g < NF ? c + g : c, w);
-        solve_lines_mx<LT, G>(lines, NF - c, lane, tab, nstart, nend, cf, refine);
+        solve_lines_mx<LT, G, REF>(lines, NF - c, lane, tab, nstart, nend, cf, REF ? 1 : 0);
     }
 }
 
@@ -153,11 +156,11 @@ __device__ __forceinline__ double pres_dev(double dr, double dT) { return (dr + 
 // ----------------------------------------------------------------------------
 // gradient pass (FIRST: reads the FP64 state, writes the shadow, reduces CFL)
 // ----------------------------------------------------------------------------
-template <int LT, int AXIS, int TL, bool FIRST>
+template <int LT, int AXIS, int TL, bool FIRST, bool REF>
 __global__ void __launch_bounds__(TL * 32, TL == 8 ? 2 : 1)
 k_grad_mx(const double *__restrict__ q, float *__restrict__ sh, float *__restrict__ g,
           DevTables<float> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf,
-          Phys ph, unsigned long long *__restrict__ dtacc, int refine) {
+          Phys ph, unsigned long long *__restrict__ dtacc) {
     using L = LineLayout<LT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *sm = reinterpret_cast<float *>(smem_raw);
@@ -200,7 +203,7 @@ k_grad_mx(const double *__restrict__ q, float *__restrict__ sh, float *__restric
         field_line32<LT, TL>(sm, 3, l)[pj] = tp;
     });
     tile_sync<AXIS, TL>();
-    if (line0 + w < F) solve_fields_mx<LT, TL, 4>(sm, w, lane, tab, nstart, nend, cf, refine);
+    if (line0 + w < F) solve_fields_mx<LT, TL, 4, REF>(sm, w, lane, tab, nstart, nend, cf);
     tile_sync<AXIS, TL>();
     tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         const int pj = L::pos(j);
@@ -269,12 +272,12 @@ __device__ __forceinline__ void point_flux_mx(const float *__restrict__ sh, cons
     for (int m = 0; m < 5; ++m) flo[m] = (float)fl[m];
 }
 
-template <int LT, int AXIS, int TL, int MODE, bool VISC, bool SHADOW_OUT>
+template <int LT, int AXIS, int TL, int MODE, bool VISC, bool SHADOW_OUT, bool REF>
 __global__ void __launch_bounds__(TL * 32, TL == 8 ? 2 : 1)
 k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__restrict__ rhs,
           const double *__restrict__ qn, double *__restrict__ qout, float *__restrict__ sh_out,
           double *__restrict__ drva, DevTables<float> tab, int lxi, int let, int64_t lmx, int64_t F,
-          int nstart, int nend, Coeffs cf, Phys ph, RkParams rk, int refine) {
+          int nstart, int nend, Coeffs cf, Phys ph, RkParams rk) {
     using L = LineLayout<LT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *sm = reinterpret_cast<float *>(smem_raw);
@@ -291,7 +294,7 @@ k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__re
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
     if (fidx < F) {
-        solve_fields_mx<LT, TL, 5>(sm, w, lane, tab, nstart, nend, cf, refine);
+        solve_fields_mx<LT, TL, 5, REF>(sm, w, lane, tab, nstart, nend, cf);
         if (drva) {
             __syncwarp();
             if (lane < 10) {
@@ -363,12 +366,13 @@ struct MixedArgs {
 template <int LT, int AXIS, int TL>
 int launch_grad_mx_t(const MixedArgs &a, const double *q, bool first, cudaStream_t st) {
     const size_t smem = (size_t)4 * TL * LineLayout<LT>::kSlot * sizeof(float);
-    auto kern = first ? k_grad_mx<LT, AXIS, TL, true> : k_grad_mx<LT, AXIS, TL, false>;
+    auto kern = first ? (a.refine ? k_grad_mx<LT, AXIS, TL, true, true> : k_grad_mx<LT, AXIS, TL, true, false>)
+                      : (a.refine ? k_grad_mx<LT, AXIS, TL, false, true> : k_grad_mx<LT, AXIS, TL, false, false>);
     if (int rc = set_smem(kern, smem)) return rc;
     const PassArgs &b = a.base;
     const unsigned blocks = (unsigned)((b.F + TL - 1) / TL);
     kern<<<blocks, TL * 32, smem, st>>>(q, a.shadow, a.grad + (int64_t)AXIS * 4 * b.lmx, b.tab->t32, b.lxi,
-                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, b.dtacc, a.refine);
+                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, b.dtacc);
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }
@@ -380,14 +384,18 @@ int launch_flux_mx_t(const MixedArgs &a, const double *qn, double *qout, bool sh
     const PassArgs &b = a.base;
     // the shadow is written only by the RK modes
     constexpr bool kRk = MODE >= kAccumRk;
-    auto kern = b.viscous ? (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, true, kRk>
-                                               : k_flux_mx<LT, AXIS, TL, MODE, true, false>)
-                          : (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, false, kRk>
-                                               : k_flux_mx<LT, AXIS, TL, MODE, false, false>);
+    auto pick = [&](auto ref) {
+        constexpr bool R = decltype(ref)::value;
+        return b.viscous ? (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, true, kRk, R>
+                                              : k_flux_mx<LT, AXIS, TL, MODE, true, false, R>)
+                         : (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, false, kRk, R>
+                                              : k_flux_mx<LT, AXIS, TL, MODE, false, false, R>);
+    };
+    auto kern = a.refine ? pick(std::true_type{}) : pick(std::false_type{});
     if (int rc = set_smem(kern, smem)) return rc;
     const unsigned blocks = (unsigned)((b.F + TL - 1) / TL);
     kern<<<blocks, TL * 32, smem, st>>>(a.shadow, a.grad, a.rhs, qn, qout, a.shadow, drva, b.tab->t32, b.lxi,
-                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, rk, a.refine);
+                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, rk);
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }
