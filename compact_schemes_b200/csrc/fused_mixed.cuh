@@ -124,11 +124,12 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
 #endif
 
 // The NF fields of this warp's line of the tile, CSB_MX_SOLVE_GROUP at a time
-// (one at a time for lines of more than 256 points: registers).
+// (one at a time for lines of more than 256 points when the refinement sweep
+// is compiled in: registers).
 template <int LT, int TL, int NF, bool REF>
 __device__ __forceinline__ void solve_fields_mx(float *sm, int w, int lane, const DevTables<float> &tab,
                                                 int nstart, int nend, const Coeffs &cf) {
-    constexpr int G = LT >= 16 ? 1 : CSB_MX_SOLVE_GROUP;
+    constexpr int G = (LT >= 16 && REF) ? 1 : CSB_MX_SOLVE_GROUP;
 #pragma unroll 1
     for (int c = 0; c < NF; c += G) {
         float *lines[G];
