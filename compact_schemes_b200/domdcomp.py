@@ -151,11 +151,22 @@ def exchange(send, recv, dd, nn, group=None):
             part(recv, ip_recv).copy_(landing)
 
 
+_P2P_READY = set()
+
+
 def mpigo(numerics, dd, variable_id, group=None):
     """numerics_base::mpigo over torch.distributed for one variable: every
     interface axis of the block exchanges the send buffers that
-    ``numerics.fill_buffers`` wrote (src/numerics_base.hpp:119-180)."""
+    ``numerics.fill_buffers`` wrote (src/numerics_base.hpp:119-180).  Every
+    rank of the group calls it, in the same order of variables."""
     import torch
+    import torch.distributed as dist
+    key = id(group)
+    if key not in _P2P_READY:
+        # the first point-to-point batch of an NCCL group must involve every
+        # rank; a barrier on the group first makes any later subset valid
+        dist.barrier(group=group)
+        _P2P_READY.add(key)
     torch.cuda.synchronize()  # the sums of fill_buffers are complete on every stream
     for nn in range(3):
         if dd.interface(0, nn) or dd.interface(1, nn):
