@@ -42,3 +42,39 @@ def test_multiblock_deriv_matches_serial_emulation(cuda, gdims, nbpc, nbc):
             assert np.abs(got - r).max() / np.abs(r).max() < 1e-12, (axis, dd.rank)
     for nm in nms:
         nm.close()
+
+
+def test_mpigo_on_a_one_rank_nccl_group_equals_self_exchange(cuda):
+    """mpigo over torch.distributed (here one NCCL rank, periodic on every
+    axis: the rank is its own neighbour) fills the recv buffers exactly as
+    the single-rank self exchange does."""
+    import datetime
+    import os
+    import socket
+    import torch
+    import torch.distributed as dist
+    import compact_schemes_b200 as cs
+    from compact_schemes_b200.domdcomp import _buffers, domdcomp, mpigo
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        gdims = (32, 24, 16)
+        dd = domdcomp(gdims, (1, 1, 1), [[P] * 3, [P] * 3], 0)
+        f = torch.from_numpy(np.random.default_rng(3).normal(size=int(np.prod(gdims)))).to(cuda)
+        a, b = cs.numerics_pc(gdims, dd.nbc), cs.numerics_pc(gdims, dd.nbc)
+        for nm in (a, b):
+            nm.deriv_setup()
+            nm.fill_buffers(f, 0, 1, 1, gdims)
+        mpigo(a, dd, 0)
+        b.mpigo(gdims, None, 1, 0)
+        torch.cuda.synchronize()
+        for nn in range(3):
+            assert torch.equal(_buffers(a, dd, nn, 0)[1], _buffers(b, dd, nn, 0)[1])
+        a.close()
+        b.close()
+    finally:
+        dist.destroy_process_group()
