@@ -59,7 +59,7 @@ def parse():
     return p.parse_args()
 
 
-def config3_section(args, steps=6):
+def mixed_512_gcbc_section(args, steps=6):
     """Mixed form of the Taylor-Green box at 512^3 with non-reflective GCBC x
     faces and periodic y/z: both forms autotuned, ms per step, and the
     per-field error of the mixed state against the FP64 state after the same
@@ -608,14 +608,14 @@ def run_ours(args):
                "sample": "1 RK stage of the %d^3 Taylor-Green box in %.1f s (FP64 oracle, "
                          "C++/OpenMP restatement of the reference kernels)" % (n, t)}
 
-    ensemble = adjoint = config3 = curvilinear = None
+    ensemble = adjoint = mixed512 = curvilinear = None
     if rank == 0 and world == 1:
         s.close()
         if not args.no_curvilinear:
             curvilinear = curvilinear_section(args, t_ms / args.steps)
             torch.cuda.empty_cache()
         if not args.no_mixed:
-            config3 = config3_section(args)
+            mixed512 = mixed_512_gcbc_section(args)
             torch.cuda.empty_cache()
         if not args.no_ensemble:
             ensemble = ensemble_section(args)
@@ -638,7 +638,7 @@ def run_ours(args):
                            "schedule": {"%s_%s" % ("grad" if k == 0 else "flux", "xyz"[a]): v
                                         for (k, a), v in tuned.items()}},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed,
-                "config3_mixed_512": config3, "ensemble": ensemble, "adjoint": adjoint,
+                "mixed_512_gcbc": mixed512, "ensemble": ensemble, "adjoint": adjoint,
                 "curvilinear": curvilinear,
                 "gpu_launches": 24 * args.steps, "clocks": clocks,
                 "passes": per_pass,

@@ -2,7 +2,7 @@
 an optional FP64-residual refinement sweep), FP64 state, RK accumulation and
 thermodynamics.
 
-Target (north star): relative state error <= 1e-6 per field after 100 RK steps
+Target: relative state error <= 1e-6 per field after 100 RK steps
 against the FP64 path.  Relative error of a field f: max|f - f64| / max|f64|.
 rho*w starts at exactly zero in the Taylor-Green state, so its relative error
 is measured against a field that is small throughout and gets a looser bound.
@@ -63,7 +63,7 @@ def test_mixed_100_steps_within_1e6(cuda, refine):
     assert errs[3] <= 1e-5, errs
 
 
-def test_config2_mixed_512_gcbc(cuda):
+def test_mixed_512_gcbc_100_steps(cuda):
     """512^3 mixed form with non-reflective GCBC on the x faces, periodic y/z,
     100 RK steps; per-field error against the FP64 path (itself checked against
     the CPU oracle at <= 256^3)."""

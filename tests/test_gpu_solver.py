@@ -1,6 +1,6 @@
 """GPU parity of the fused RHS / RK pipeline against the FP64 oracle.
 
-Tolerances (north_star): 1e-12 relative max-norm per RHS field,
+Tolerances: 1e-12 relative max-norm per RHS field,
 1e-10 after 100 RK steps.  Relative max-norm of a field f:
 max|f - f_oracle| / max|f_oracle|.
 """
