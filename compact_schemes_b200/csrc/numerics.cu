@@ -229,6 +229,96 @@ k_deriv(const T *__restrict__ in, T *__restrict__ out, DevTables<T> tab, int lxi
     store_tile<LT, AXIS>(out, sm, line0, F, n, lxi, let);
 }
 
+// Same derivative with two lines per warp: a CTA of kThreads threads holds
+// kPairLines lines, warp w solves lines 2w and 2w+1 in one warp_solve (their
+// table loads and shuffle latencies are shared), and the y/z tiles cover 16
+// consecutive x positions (128-byte rows).  Used for chunks of up to 8 rows.
+constexpr int kPairLines = 16;
+#ifndef CSB_PAIR_MINB
+#define CSB_PAIR_MINB 3
+#endif
+
+template <int LT, int AXIS, typename T, bool STORE>
+__device__ __forceinline__ void pair_tile_io(const T *__restrict__ in, T *__restrict__ out, T *sm, int64_t line0,
+                                             int64_t F, int n, int lxi, int let) {
+    using L = LineLayout<LT>;
+    const int tid = threadIdx.x;
+    if (AXIS == 0) {
+        const int w = tid >> 5, lane = tid & 31;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int l = 2 * w + h;
+            const int64_t fidx = line0 + l;
+            if (fidx >= F) continue;
+            for (int j = lane; j < n; j += 32) {
+                if (STORE) out[fidx * n + j] = sm[l * L::kSlot + L::pos(j)];
+                else sm[l * L::kSlot + L::pos(j)] = in[fidx * n + j];
+            }
+        }
+    } else {
+        const int l = tid % kPairLines;
+        const int64_t fidx = line0 + l;
+        if (fidx < F) {
+            const int64_t base = line_base<AXIS>(fidx, lxi, let), s = line_stride<AXIS>(lxi, let);
+            for (int j = tid / kPairLines; j < n; j += kThreads / kPairLines) {
+                if (STORE) out[base + j * s] = sm[l * L::kSlot + L::pos(j)];
+                else sm[l * L::kSlot + L::pos(j)] = in[base + j * s];
+            }
+        }
+    }
+}
+
+template <int LT, int AXIS, typename T>
+__global__ void __launch_bounds__(kThreads, CSB_PAIR_MINB)
+k_deriv_pair(const T *__restrict__ in, T *__restrict__ out, DevTables<T> tab, int lxi, int let, int nstart,
+             int nend, const T *__restrict__ recv, T *__restrict__ drva, int64_t F, Coeffs cf) {
+    using L = LineLayout<LT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sm = reinterpret_cast<T *>(smem_raw);
+    const int n = tab.n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t line0 = (int64_t)blockIdx.x * kPairLines;
+    pair_tile_io<LT, AXIS, T, false>(in, nullptr, sm, line0, F, n, lxi, let);
+    if (AXIS == 0) __syncwarp();
+    else __syncthreads();
+    const int64_t fidx0 = line0 + 2 * w;
+    if (fidx0 < F) {
+        T d[2][LT];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t fidx = fidx0 + h;
+            if (fidx < F) {
+                T r4[4];
+                const T *rp = nullptr;
+                if (recv && (nstart || nend)) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) r4[k] = recv[k * F + fidx];
+                    rp = r4;
+                }
+                deriv_rhs<LT, T, T>(sm + (2 * w + h) * L::kSlot, n, lane, nstart, nend, rp, cf, d[h]);
+            } else {
+#pragma unroll
+                for (int t = 0; t < LT; ++t) d[h][t] = T(0);
+            }
+        }
+        warp_solve<LT, 2, T>(tab, d, lane);
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t fidx = fidx0 + h;
+            if (fidx >= F) continue;
+            if (drva) {
+                if (lane == 0) drva[fidx] = d[h][0];
+                if (lane == (n - 1) / LT) drva[5 * F + fidx] = get_at<LT, T>(d[h], (n - 1) - lane * LT);
+            }
+            store_line_regs<LT, T>(sm + (2 * w + h) * L::kSlot, d[h], lane, n);
+        }
+    }
+    if (AXIS == 0) __syncwarp();
+    else __syncthreads();
+    pair_tile_io<LT, AXIS, T, true>(nullptr, out, sm, line0, F, n, lxi, let);
+}
+
 // Compact filter of one field along AXIS.
 template <int LT, int AXIS>
 __global__ void __launch_bounds__(kThreads)
@@ -299,6 +389,16 @@ static int launch_deriv_lt(const T *in, T *out, const DevTables<T> &tab, const c
                            int nstart, int nend, const T *recv, T *drva, const Coeffs &cf,
                            cudaStream_t st) {
     const int64_t F = face_size(d, AXIS);
+    if constexpr (LT <= 8) {
+        const size_t smem = (size_t)kPairLines * LineLayout<LT>::kSlot * sizeof(T);
+        auto kern = k_deriv_pair<LT, AXIS, T>;
+        if (int rc = prep_smem(kern, smem)) return rc;
+        const int64_t blocks = (F + kPairLines - 1) / kPairLines;
+        kern<<<(unsigned)blocks, kThreads, smem, st>>>(in, out, tab, d.lxi, d.let, nstart, nend, recv, drva, F,
+                                                      cf);
+        CSB_CUDA(cudaGetLastError());
+        return CS_OK;
+    }
     const size_t smem = (size_t)kTileLines * LineLayout<LT>::kSlot * sizeof(T);
     auto kern = k_deriv<LT, AXIS, T>;
     int rc = prep_smem(kern, smem);
