@@ -56,6 +56,9 @@ def parse():
     p.add_argument("--no-ensemble", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-curvilinear", action="store_true")
+    p.add_argument("--no-reference-kernels", action="store_true")
+    p.add_argument("--no-config1", action="store_true")
+    p.add_argument("--no-dropin", action="store_true")
     return p.parse_args()
 
 
@@ -330,6 +333,262 @@ def _adjoint_map(a, s, q0, dts, every, y, lam_out):
     return True
 
 
+REF_GPU = os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so")
+
+
+class _Raw:
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3}
+
+
+def device_view(ptr, n):
+    """torch float64 view of n doubles at a raw device address owned by the library."""
+    import torch
+    return torch.as_tensor(_Raw(ptr, n), device="cuda")
+
+
+def reference_kernels_section(args):
+    """The reference's own sm_100a kernels for the derivative and flux steps,
+    compiled from its sources into oracle/_ref/libref_gpu.so, timed beside
+    this library's on the same 256^3 FP64 inputs (CUDA events, one stream,
+    after warm-up; inputs larger than L2):
+      deriv_kernel_2d<Axis,double> (src/cuda/kernels/numerics_pc.hpp:174-249)
+        against cs_deriv, y and z lines, physical (ndf 0) and periodic (ndf 1)
+        closures; 16 B/pt (one field read, one written).  The reference's x
+        kernel is valid only for lze = 1 and is not timed;
+      calc_fluxes_pre_compute_kernel<true,double>
+        (src/cuda/kernels/physics.hpp:42-193) against cs_calc_fluxes_pre:
+        reads qa 5, p, de 5, metrics 9, tau 6, heat 3, writes 15 fluxes and
+        de[4]: 45 words = 360 B/pt."""
+    import ctypes
+    import torch
+    import compact_schemes_b200 as cs
+    if not os.path.exists(REF_GPU):
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built (make -C oracle ref needs the reference sources)"}
+    R = ctypes.CDLL(REF_GPU)
+    vp = ctypes.c_void_p
+    R.ref_gpu_deriv2d.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_uint, vp]
+    R.ref_gpu_fluxes_pre_time.argtypes = [vp] * 9 + [ctypes.c_double] * 3 + [ctypes.c_uint, vp, ctypes.c_int, vp,
+                                                                             ctypes.POINTER(ctypes.c_float)]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    sp = vp(stream.cuda_stream)
+    reps, warm = 20, 3
+    hbm, _ = peaks()
+    n = 256
+    dims = (n, n, n)
+    lmx = n ** 3
+
+    def timed(fn):
+        for _ in range(warm):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    rows = []
+    for axis in (1, 2):
+        for ndf in (0, 1):
+            b = cs.BC_PERIODIC if ndf else cs.BC_NON_REFLECTIVE
+            nm = cs.numerics_pc(dims, [[b] * 3] * 2)
+            nm.deriv_setup()
+            g = torch.Generator(device=dev).manual_seed(1)
+            f = torch.randn(lmx, dtype=torch.float64, device=dev, generator=g)
+            if ndf:
+                blk = torch.zeros(15 * lmx, dtype=torch.float64, device=dev)
+                blk[axis * lmx:(axis + 1) * lmx] = f
+                nm.fill_buffers(blk, 0, 1, 0, dims)
+                nm.mpigo(dims, None, 1, 0)
+                del blk
+            ours = torch.empty(3 * lmx, dtype=torch.float64, device=dev)
+            theirs = torch.empty(3 * lmx, dtype=torch.float64, device=dev)
+            _, _, recv = nm.buffers(axis)
+            scratch = torch.zeros(10 * n * n, dtype=torch.float64, device=dev)
+            _, pbci = nm.coeffs()
+            dpbci = torch.tensor(pbci, dtype=torch.float64, device=dev)
+            t_ours = timed(lambda: nm.deriv2d(axis, f, ours, ndf, ndf, dims, 0, 0, stream=stream))
+
+            def run_ref():
+                rc = R.ref_gpu_deriv2d(axis, vp(f.data_ptr()), vp(theirs.data_ptr()), vp(recv),
+                                       vp(dpbci.data_ptr()), vp(scratch.data_ptr()), ndf, ndf, *dims, 0, 0, sp)
+                if rc:
+                    raise RuntimeError("reference deriv kernel launch failed: %d" % rc)
+            t_ref = timed(run_ref)
+            a, t = ours[axis * lmx:(axis + 1) * lmx], theirs[axis * lmx:(axis + 1) * lmx]
+            gbs = lambda ms: 16.0 * lmx / (ms * 1e-3) / 1e9
+            rows.append({"kernel": "deriv", "axis": "xyz"[axis], "ndf": ndf, "ours_ms": t_ours,
+                         "reference_ms": t_ref, "speedup": t_ref / t_ours, "ours_frac": gbs(t_ours) / hbm,
+                         "reference_frac": gbs(t_ref) / hbm,
+                         "max_rel_diff": float((a - t).abs().max() / t.abs().max())})
+            nm.close()
+            del f, ours, theirs, scratch
+            torch.cuda.empty_cache()
+    # flux pre-compute on a smooth state with per-point metrics
+    g = torch.Generator(device=dev).manual_seed(2)
+    rnd = lambda k: torch.rand(k * lmx, dtype=torch.float64, device=dev, generator=g)
+    rho = 1.0 + 0.1 * rnd(1)
+    vel = 0.3 * (rnd(3) - 0.5)
+    p = 1 / 1.4 + 0.05 * rnd(1)
+    v3 = vel.view(3, -1)
+    qa = torch.cat([rho, rho * v3[0], rho * v3[1], rho * v3[2], p / 0.4 + 0.5 * rho * (v3 ** 2).sum(0)])
+    de = torch.cat([1 / rho, v3[0], v3[1], v3[2], 1.4 * p / rho])
+    h = 2 * math.pi / n
+    met = [torch.zeros(3 * lmx, dtype=torch.float64, device=dev) for _ in range(3)]
+    for a in range(3):
+        met[a][a * lmx:(a + 1) * lmx] = h * h * (1 + 0.01 * rnd(1))
+    tau, heat = 1e-3 * rnd(6), 1e-3 * rnd(3)
+    ph = cs.physics(dims, True)
+    ph.umf = (0.0, 0.0, 0.0)
+    b0, _, dtau, dheat = ph.buffers()
+    device_view(dtau, 6 * lmx).copy_(tau)
+    device_view(dheat, 3 * lmx).copy_(heat)
+    de_o = de.clone()
+    t_ours = timed(lambda: ph.calc_fluxes_pre(qa, p, de_o, met[0], met[1], met[2], stream=stream))
+    theirs = torch.zeros(15 * lmx, dtype=torch.float64, device=dev)
+    de_r = de.clone()
+    structs = torch.zeros(16, dtype=torch.float64, device=dev)
+    ms = ctypes.c_float()
+    ptrs = [vp(x.data_ptr()) for x in (theirs, qa, p, de_r, met[0], met[1], met[2], tau, heat)]
+    for _ in range(2):
+        rc = R.ref_gpu_fluxes_pre_time(*ptrs, 0.0, 0.0, 0.0, lmx, vp(structs.data_ptr()), warm, sp, ctypes.byref(ms))
+    rc = R.ref_gpu_fluxes_pre_time(*ptrs, 0.0, 0.0, 0.0, lmx, vp(structs.data_ptr()), reps, sp, ctypes.byref(ms))
+    if rc:
+        raise RuntimeError("reference flux kernel failed: %d" % rc)
+    t_ref = float(ms.value)
+    torch.cuda.synchronize()
+    ours_buf = device_view(b0, 15 * lmx)
+    diff = max(float((ours_buf[c * lmx:(c + 1) * lmx] - theirs[c * lmx:(c + 1) * lmx]).abs().max() /
+                     theirs[c * lmx:(c + 1) * lmx].abs().max()) for c in range(15))
+    gbs = lambda ms_: 360.0 * lmx / (ms_ * 1e-3) / 1e9
+    rows.append({"kernel": "fluxes_pre", "ours_ms": t_ours, "reference_ms": t_ref, "speedup": t_ref / t_ours,
+                 "ours_frac": gbs(t_ours) / hbm, "reference_frac": gbs(t_ref) / hbm, "max_rel_diff": diff})
+    ph.close()
+    del qa, de, de_o, de_r, met, tau, heat, theirs
+    torch.cuda.empty_cache()
+    return {"workload": "256^3 FP64 fields, one launch per kernel", "reps": reps,
+            "deriv_bytes_per_point": 16, "fluxes_pre_bytes_per_point": 360, "rows": rows}
+
+
+def dropin_section(args, fused_ms_per_step, stages=8):
+    """The reference-shaped call sequence through the drop-in API, the path a
+    caller of physics / numerics_pc gets: per RK stage thermo,
+    calc_viscous_shear_stress, thermo, calc_fluxes (15 single-field solves
+    plus the interface sums) and rk_update, on the 256^3 Taylor-Green state
+    with per-point metric arrays of the uniform grid.  Unfused pointwise
+    kernels; timed with CUDA events over `stages` stages."""
+    import torch
+    import compact_schemes_b200 as cs
+    n = args.n
+    dims = (n, n, n)
+    lmx = n ** 3
+    dev = torch.device("cuda", torch.cuda.current_device())
+    nbc = [[cs.BC_PERIODIC] * 3] * 2
+    nm = cs.numerics_pc(dims, nbc)
+    nm.deriv_setup()
+    ph = cs.physics(dims, True)
+    q = torch.empty(5 * lmx, dtype=torch.float64, device=dev)
+    cs.tgv_init(q, dims, MACH, 1e-4, 0)
+    qn = q.clone()
+    h = 2 * math.pi / n
+    met = [torch.zeros(3 * lmx, dtype=torch.float64, device=dev) for _ in range(3)]
+    for a in range(3):
+        met[a][a * lmx:(a + 1) * lmx] = h * h
+    yaco = torch.full((lmx,), 1.0 / h ** 3, dtype=torch.float64, device=dev)
+    de = torch.zeros(5 * lmx, dtype=torch.float64, device=dev)
+    p = torch.zeros(lmx, dtype=torch.float64, device=dev)
+    ssk = torch.full((lmx,), MACH / RE, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+    dt = 1e-3
+
+    def stage(k):
+        cs.thermo(q, de, p, stream=stream)
+        ph.calc_viscous_shear_stress(de, ssk, met[0], met[1], met[2], yaco, dims, None, nm, streams=stream)
+        cs.thermo(q, de, p, stream=stream)
+        ph.calc_fluxes(q, p, de, met[0], met[1], met[2], dims, None, nm, streams=stream)
+        cs.rk_update(qn, de, yaco, dt / (4 - k % 4), q, stream=stream)
+
+    for k in range(2):
+        stage(k)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(stages):
+        stage(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / stages
+    ph.close()
+    nm.close()
+    del q, qn, met, yaco, de, p, ssk
+    torch.cuda.empty_cache()
+    return {"workload": "256^3 Taylor-Green, FP64, drop-in physics / numerics_pc call sequence per RK stage "
+                        "(metric arrays of the uniform grid)",
+            "value": lmx / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_stage": ms,
+            "fused_ms_per_stage": fused_ms_per_step / 4, "fused_speedup": ms / (fused_ms_per_step / 4),
+            "stages": stages}
+
+
+def config1_section(args, reps=20):
+    """The derivative-and-filter workload: the 64^3 non-periodic [0,1]^3
+    field of 8 Fourier modes (MT19937-64 seed 0), physical closures on all
+    faces; index-space compact derivatives along x, y, z and the filter
+    (alpha_f 0.45) along x then y then z.  GPU: 6 line-solve launches per
+    pass (the field is L2-resident, 2 MB: latency-bound, not an HBM case);
+    CPU: the oracle on the host cores.  Error: GPU against the oracle."""
+    import numpy as np
+    import torch
+    import compact_schemes_b200 as cs
+    import oracle as O
+    dims = (64, 64, 64)
+    nm = cs.numerics_pc(dims, [[cs.BC_NON_REFLECTIVE] * 3] * 2)
+    nm.deriv_setup()
+    f = cs.grid.fourier_field(dims, 0, 8)
+    d = [torch.empty_like(f) for _ in range(3)]
+    a, b = torch.empty_like(f), torch.empty_like(f)
+    stream = torch.cuda.current_stream()
+
+    def gpu_pass():
+        for ax in range(3):
+            nm.deriv1d(ax, f, d[ax], 0, 0, dims, 0, halo=cs.HALO_SELF, stream=stream)
+        nm.filter(0, f, a, 0.45, dims, stream=stream)
+        nm.filter(1, a, b, 0.45, dims, stream=stream)
+        nm.filter(2, b, a, 0.45, dims, stream=stream)
+
+    for _ in range(3):
+        gpu_pass()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        gpu_pass()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    gpu_ms = e0.elapsed_time(e1) / reps
+    fh = f.cpu().numpy()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        ref_d = [O.deriv(fh, dims, ax, 0, 0) for ax in range(3)]
+        r = fh
+        for ax in range(3):
+            r = O.filt(r, dims, ax, 0, 0, 0.45)
+    cpu_ms = (time.perf_counter() - t0) * 1e3 / 3
+    rel = lambda x, y: float(np.abs(x - y).max() / np.abs(y).max())
+    errs = {"deriv_" + "xyz"[ax]: rel(d[ax].cpu().numpy(), ref_d[ax]) for ax in range(3)}
+    errs["filter_xyz"] = rel(a.cpu().numpy(), r)
+    nm.close()
+    return {"workload": "64^3 Fourier-mode field (8 modes, MT19937-64 seed 0), non-periodic [0,1]^3: "
+                        "d/dx, d/dy, d/dz and filter x->y->z", "gpu_ms_per_pass": gpu_ms,
+            "cpu_ms_per_pass": cpu_ms, "cpu_cores": O.num_threads(), "cpu_kind": "port (FP64 oracle)",
+            "speedup_gpu_vs_cpu": cpu_ms / gpu_ms, "rel_err_gpu_vs_oracle": errs, "tolerance": 1e-12}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -442,6 +701,14 @@ def cpu_oracle_stage_rate(n, stages=1):
     return n ** 3 * stages / t / 1e6, t, O.num_threads()
 
 
+def workload_config(n, world):
+    """The workload both arms print (the same keys and values)."""
+    return {"workload": "taylor_green_%d^3_fp64_plain" % n, "n": n, "mach": MACH, "re": RE, "cfl": CFL,
+            "rk": "4-stage, q^(k) = q^n - dt/(4-k) J R", "bc": "periodic (quasi-disjoint closure)",
+            "l2": "inputs larger than L2 (state 671 MB + gradients 1.6 GB), no flush",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
+
+
 def run_reference(args):
     """Reference arm: the reference has no CPU implementation of the path, so its
     CPU path is the oracle port of its kernels, timed on the host cores."""
@@ -472,11 +739,11 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "taylor_green_256^3_fp64_plain", "n": n, "step": "one RK stage",
-                       "mach": MACH, "re": RE, "cfl": CFL},
+            "config": workload_config(n, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": "%d RK stages of the %d^3 Taylor-Green box (FP64 oracle, "
-                                       "C++/OpenMP restatement of the reference kernels)" % (args.steps, n)},
+                                       "C++/OpenMP restatement of the reference kernels; a step of this "
+                                       "arm is one RK stage, dt from the initial state)" % (args.steps, n)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -527,25 +794,35 @@ def run_ours(args):
     per_pass = {}
     for k, (ms, cnt) in prof.items():
         if cnt:
+            b = ALG_BYTES.get(k)
+            if k == "flux_z_rk":  # stage 0 reads q^n only once: stage-averaged bytes
+                b = (3 * ALG_BYTES[k] + (ALG_BYTES[k] - 40)) / 4
             per_pass[k] = {"ms_per_launch": ms / cnt, "launches": cnt, "total_ms": ms}
+            if b:
+                gbs = b * lmx / (ms / cnt * 1e-3) / 1e9
+                per_pass[k].update({"alg_bytes_per_point": b, "achieved_gbs": gbs, "frac": gbs / hbm})
     top = max(per_pass, key=lambda k: per_pass[k]["total_ms"])
-    alg = ALG_BYTES[top] * lmx
-    if top == "flux_z_rk":  # stage 0 reads q^n only once
-        alg = (3 * ALG_BYTES[top] + (ALG_BYTES[top] - 40)) / 4 * lmx
+    alg = per_pass[top]["alg_bytes_per_point"] * lmx
     achieved = alg / (per_pass[top]["ms_per_launch"] * 1e-3) / 1e9
     stage_ms = sum(v["total_ms"] for v in per_pass.values()) / (4 * args.steps)
-    traffic = None
+    traffic, traffic_src = None, None
     try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+        # DRAM bytes of one launch per stage kind of this pass at 256^3
+        # (ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/)
+        with open(os.path.join(ROOT, "profiles", "traffic_%s_256.json" % top)) as f:
             tj = json.load(f)
-        if top in tj:
-            traffic = tj[top]["bytes_per_point"] * lmx
+        if n == 256:
+            traffic = (tj["stage0_bytes"] + 3 * tj["stage1_bytes"]) / 4
+            traffic_src = {"file": "profiles/traffic_%s_256.json" % top, "stage0_bytes": tj["stage0_bytes"],
+                           "stage1_bytes": tj["stage1_bytes"],
+                           "stage0_alg_bytes": (ALG_BYTES[top] - 40) * lmx if top == "flux_z_rk" else None,
+                           "stage1_alg_bytes": ALG_BYTES[top] * lmx}
     except Exception:
         pass
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "kernel": top,
                 "peak_source": peak_kind,
-                "alg_bytes_per_launch": alg}
+                "alg_bytes_per_launch": alg, "traffic_detail": traffic_src}
 
     # --- e2e: host buffers through cs_solver_step_host ------------------------------
     qh_in = torch.empty(5 * lmx, dtype=torch.float64, pin_memory=True)
@@ -608,9 +885,17 @@ def run_ours(args):
                "sample": "1 RK stage of the %d^3 Taylor-Green box in %.1f s (FP64 oracle, "
                          "C++/OpenMP restatement of the reference kernels)" % (n, t)}
 
-    ensemble = adjoint = mixed512 = curvilinear = None
+    ensemble = adjoint = mixed512 = curvilinear = refk = cfg1 = dropin = None
     if rank == 0 and world == 1:
         s.close()
+        if not args.no_reference_kernels:
+            refk = reference_kernels_section(args)
+            torch.cuda.empty_cache()
+        if not args.no_config1:
+            cfg1 = config1_section(args)
+        if not args.no_dropin:
+            dropin = dropin_section(args, t_ms / args.steps)
+            torch.cuda.empty_cache()
         if not args.no_curvilinear:
             curvilinear = curvilinear_section(args, t_ms / args.steps)
             torch.cuda.empty_cache()
@@ -629,17 +914,12 @@ def run_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
-                "config": {"workload": "taylor_green_256^3_fp64_plain" if n == 256 else
-                           "taylor_green_%d^3_fp64_plain" % n,
-                           "n": n, "mach": MACH, "re": RE, "cfl": CFL, "dt": "CFL, every step, on device",
-                           "rk": "4-stage, q^(k) = q^n - dt/(4-k) J R", "bc": "periodic (quasi-disjoint closure)",
-                           "l2": "inputs larger than L2 (state 671 MB + gradients 1.6 GB), no flush",
-                           "parallelism": "replicas" if world > 1 else "single GPU",
-                           "schedule": {"%s_%s" % ("grad" if k == 0 else "flux", "xyz"[a]): v
-                                        for (k, a), v in tuned.items()}},
+                "config": workload_config(n, world),
+                "schedule": {"%s_%s" % ("grad" if k == 0 else "flux", "xyz"[a]): v for (k, a), v in tuned.items()},
+                "dt_policy": "CFL 0.5 recomputed from q^n every step, on the device",
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed,
                 "mixed_512_gcbc": mixed512, "ensemble": ensemble, "adjoint": adjoint,
-                "curvilinear": curvilinear,
+                "curvilinear": curvilinear, "reference_kernels": refk, "config1": cfg1, "dropin": dropin,
                 "gpu_launches": 24 * args.steps, "clocks": clocks,
                 "passes": per_pass,
                 "stage_model": {"bytes_per_point": STAGE_BYTES, "ms_per_stage": stage_ms,

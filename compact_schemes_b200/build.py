@@ -11,7 +11,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcompact_b200.so")
-EXTRA = []  # extra nvcc flags (-D knobs) for tuning builds
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
@@ -35,7 +34,7 @@ def _compile(src, verbose_regs=False):
     if (os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(path)
             and os.path.getmtime(obj) >= _headers_mtime() and not verbose_regs):
         return obj, ""
-    cmd = [NVCC, *ARCH, *FLAGS, *EXTRA, "-c", "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, "-c", "-o", obj]
     if src.endswith(".cpp"):
         cmd += ["-x", "cu"]
     if verbose_regs:
@@ -47,16 +46,9 @@ def _compile(src, verbose_regs=False):
     return obj, r.stderr
 
 
-def build(verbose_regs=False, quiet=True, extra=None, build_dir=None, lib=None):
-    """Compile and link; `extra`/`build_dir`/`lib` build a variant elsewhere (tuning)."""
-    global EXTRA, BUILD, LIB
-    saved = (EXTRA, BUILD, LIB)
-    if extra is not None:
-        EXTRA, BUILD, LIB = list(extra), build_dir, lib
-    try:
-        return _build(verbose_regs, quiet)
-    finally:
-        EXTRA, BUILD, LIB = saved
+def build(verbose_regs=False, quiet=True):
+    """Compile every source that changed and link libcompact_b200.so."""
+    return _build(verbose_regs, quiet)
 
 
 def _build(verbose_regs, quiet):

@@ -56,3 +56,36 @@ def metrics(numerics, xyz, period=None, stream=None):
     check(lib().cs_grid_metrics(numerics.handle, ptr(xyz), per if per is None else ctypes.byref(per),
                                 ptr(xim), ptr(etm), ptr(zem), ptr(yaco), stream_ptr(stream)))
     return xim, etm, zem, yaco
+
+
+def fourier_modes(seed=0, nmodes=8):
+    """Modes [(A, kx, ky, kz, phi)] of the derivative-and-filter test field,
+    drawn from MT19937-64 seeded `seed`, per mode in the order A, kx, ky, kz,
+    phi, each from u = (top 53 bits of one draw) * 2^-53: A = 0.1 + 0.9 u,
+    k = 1 + floor(8 u), phi = 2 pi u."""
+    import math as _m
+    from .ensemble import MT19937_64
+    g = MT19937_64(seed)
+    out = []
+    for _ in range(nmodes):
+        a = 0.1 + 0.9 * g.uniform()
+        k = [1.0 + _m.floor(8.0 * g.uniform()) for _ in range(3)]
+        out.append((a, k[0], k[1], k[2], 2.0 * _m.pi * g.uniform()))
+    return out
+
+
+def fourier_field(dims, seed=0, nmodes=8, device="cuda"):
+    """f = sum_m A_m sin(2 pi (kx x + ky y + kz z) + phi_m) on the non-periodic
+    unit cube, x = i / (lxi - 1) (and y, z alike), as a float64 tensor [lmx]
+    in the reference's layout (x fastest)."""
+    import math as _m
+    import torch
+    lxi, let, lze = dims
+    dt = torch.float64
+    x = (torch.arange(lxi, dtype=dt, device=device) * (1.0 / (lxi - 1))).view(1, 1, lxi)
+    y = (torch.arange(let, dtype=dt, device=device) * (1.0 / (let - 1))).view(1, let, 1)
+    z = (torch.arange(lze, dtype=dt, device=device) * (1.0 / (lze - 1))).view(lze, 1, 1)
+    f = torch.zeros((lze, let, lxi), dtype=dt, device=device)
+    for a, kx, ky, kz, ph in fourier_modes(seed, nmodes):
+        f += a * torch.sin(2.0 * _m.pi * (kx * x + ky * y + kz * z) + ph)
+    return f.reshape(-1)

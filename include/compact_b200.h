@@ -104,8 +104,14 @@ int cs_deriv(cs_numerics *nm, int axis, const double *in, double *out, int nstar
  * Interface faces (nstart/nend = 1) use the single-rank periodic closure; no
  * line-end values are stored.  The first call on a device looks the array's
  * address up (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls share the array and each rewrites it: calls that may
- * overlap on the GPU (different streams, no ordering) race. */
+ * capture.  With CUDA's lazy module loading (the default), that first call,
+ * and the first call for each chunk length (lines up to 64, 128, 256, 512,
+ * 1024 points), may also load the kernel's module, which can allocate and
+ * synchronize inside the CUDA runtime: make a warm-up call with each line
+ * length before the loop that must not allocate (or set
+ * CUDA_MODULE_LOADING=EAGER).  All calls share the array and each rewrites
+ * it: calls that may overlap on the GPU (different streams, no ordering)
+ * race; calls on one stream are ordered. */
 int cs_deriv_noalloc(int axis, const double *in, double *out, int nstart, int nend, cs_dcomp d,
                      void *stream);
 /* Same for numerics_pc<float>: FP32 data and arithmetic. */
@@ -124,7 +130,7 @@ int cs_fill_buffers(cs_numerics *nm, const double *in, int var_lo, int var_hi, i
 int cs_halo_exchange_self(cs_numerics *nm, unsigned var, void *stream);
 
 /* Compact filter along `axis` (no reference implementation: the sixth-order
- * tridiagonal filter of Gaitonde & Visbal).  ndf faces of the
+ * tridiagonal filter of Gaitonde & Visbal, AIAA J. 38 (2000)).  ndf faces of the
  * axis both 1: cyclic; both 0: reduced-order boundary closure. */
 int cs_filter(cs_numerics *nm, int axis, const double *in, double *out, double alpha_f,
               cs_dcomp d, void *stream);

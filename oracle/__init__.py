@@ -73,6 +73,7 @@ def lib():
         L.or_grid_metrics.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp, vp, vp]
         L.or_grid_metrics.restype = i32
         L.or_tgv_init.argtypes = [vp, i32, i32, i32, f64, f64, ctypes.c_uint64]
+        L.or_fourier_field.argtypes = [i32, i32, i32, ctypes.c_uint64, i32, vp, vp]
         L.or_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.or_noise.restype = f64
         L.or_num_threads.restype = i32
@@ -276,6 +277,15 @@ def tgv_init(dims, mach=0.1, noise=1e-4, seed=0):
     q = np.zeros(5 * lxi * let * lze)
     lib().or_tgv_init(_p(q), lxi, let, lze, mach, noise, seed)
     return q
+
+
+def fourier_field(dims, seed=0, nmodes=8):
+    """(modes [nmodes][5] = A, kx, ky, kz, phi; field) of or_fourier_field."""
+    lxi, let, lze = dims
+    modes = np.zeros(nmodes * 5)
+    f = np.zeros(lxi * let * lze)
+    lib().or_fourier_field(lxi, let, lze, seed, nmodes, _p(modes), _p(f))
+    return modes.reshape(nmodes, 5), f
 
 
 def noise(seed, index):

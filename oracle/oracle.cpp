@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <random>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -843,6 +844,34 @@ double or_noise(uint64_t seed, uint64_t index) {
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     z = z ^ (z >> 31);
     return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+void or_fourier_field(int lxi, int let, int lze, uint64_t seed, int nmodes, double *modes, double *f) {
+    const double two_pi = 6.283185307179586476925286766559;
+    std::mt19937_64 g(seed);
+    auto u = [&g]() { return (double)(g() >> 11) * (1.0 / 9007199254740992.0); };
+    std::vector<double> m((size_t)nmodes * 5);
+    for (int k = 0; k < nmodes; ++k) {
+        double *r = &m[(size_t)k * 5];
+        r[0] = 0.1 + 0.9 * u();
+        for (int a = 1; a <= 3; ++a) r[a] = 1.0 + std::floor(8.0 * u());
+        r[4] = two_pi * u();
+    }
+    if (modes) std::memcpy(modes, m.data(), m.size() * sizeof(double));
+    if (!f) return;
+    const int64_t n = (int64_t)lxi * let * lze;
+    const double hx = 1.0 / (lxi - 1), hy = 1.0 / (let - 1), hz = 1.0 / (lze - 1);
+#pragma omp parallel for
+    for (int64_t idx = 0; idx < n; ++idx) {
+        const int64_t i = idx % lxi, j = (idx / lxi) % let, k = idx / ((int64_t)lxi * let);
+        const double x = i * hx, y = j * hy, z = k * hz;
+        double s = 0.0;
+        for (int q = 0; q < nmodes; ++q) {
+            const double *r = &m[(size_t)q * 5];
+            s += r[0] * std::sin(two_pi * (r[1] * x + r[2] * y + r[3] * z) + r[4]);
+        }
+        f[idx] = s;
+    }
 }
 
 void or_tgv_init(double *q, int lxi, int let, int lze, double mach, double amp, uint64_t seed) {

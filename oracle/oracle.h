@@ -144,6 +144,14 @@ void or_tgv_init(double *q, int lxi, int let, int lze, double mach, double noise
                  uint64_t seed);
 double or_noise(uint64_t seed, uint64_t index);
 
+/* The derivative-and-filter test field on the non-periodic unit cube
+ * (x = i/(lxi-1), ...): f = sum_m A_m sin(2 pi (kx x + ky y + kz z) + phi_m)
+ * over nmodes modes drawn from std::mt19937_64(seed), per mode in the order
+ * A, kx, ky, kz, phi, each from u = (top 53 bits of one draw) * 2^-53:
+ * A = 0.1 + 0.9 u, k = 1 + floor(8 u), phi = 2 pi u.  modes: [nmodes][5]
+ * (A, kx, ky, kz, phi), may be NULL; f: [lxi*let*lze], may be NULL. */
+void or_fourier_field(int lxi, int let, int lze, uint64_t seed, int nmodes, double *modes, double *f);
+
 /* Solve every line bottom-up instead of top-down (same mathematics, other
  * rounding): the oracle against itself in this mode measures the FP64 noise
  * floor of a quantity. */

@@ -59,3 +59,36 @@ extern "C" int ref_gpu_fluxes_pre(double *buffer, double *qa, double *p, double 
     cudaStreamSynchronize(s);
     return (int)cudaGetLastError();
 }
+
+/* Timing of the reference's flux pre-compute kernel: the stress / heat-flux
+ * pointer structs are uploaded once, then `reps` launches on `stream` are
+ * bracketed by CUDA events; *ms = average milliseconds per launch. */
+extern "C" int ref_gpu_fluxes_pre_time(double *buffer, double *qa, double *p, double *de, double *xim,
+                                       double *etm, double *zem, double *tau6, double *heat3, double umfx,
+                                       double umfy, double umfz, unsigned n, void *structs, int reps,
+                                       void *stream, float *ms) {
+    cudaStream_t s = (cudaStream_t)stream;
+    t_stress_tensor<double> st{tau6, tau6 + n, tau6 + 2 * (size_t)n, tau6 + 3 * (size_t)n,
+                               tau6 + 4 * (size_t)n, tau6 + 5 * (size_t)n};
+    t_heat_fluxes<double> hf{heat3, heat3 + n, heat3 + 2 * (size_t)n};
+    auto *dst = (t_stress_tensor<double> *)structs;
+    auto *dhf = (t_heat_fluxes<double> *)((char *)structs + sizeof(st));
+    cudaMemcpyAsync(dst, &st, sizeof st, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dhf, &hf, sizeof hf, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    t_point<double> umf{umfx, umfy, umfz};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps; ++r)
+        calc_fluxes_pre_compute_kernel<true, double><<<(n + 255) / 256, 256, 0, s>>>(
+            buffer, qa, p, de, xim, etm, zem, dst, dhf, umf, n);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    *ms /= reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (int)cudaGetLastError();
+}

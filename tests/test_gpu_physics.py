@@ -172,3 +172,58 @@ def test_wall_condition_update_matches_oracle(cuda, nbc):
     got = qd.cpu().numpy()
     assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()
     assert not np.array_equal(ref, q)  # some wall points changed
+
+
+REF_GPU = os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference kernels not built (make -C oracle ref)")
+def test_fluxes_pre_against_reference_fp64_kernel(cuda):
+    """The reference's own calc_fluxes_pre_compute_kernel<true,double>
+    (src/cuda/kernels/physics.hpp:42-193), compiled for sm_100a from its
+    sources, against cs_calc_fluxes_pre on the same FP64 inputs: a 64^3
+    state, per-point metrics, stress tensor and heat flux, moving frame.
+    1e-12 relative max-norm per flux component; the reference lets the
+    compiler contract products into FMAs, so last bits differ."""
+    import ctypes
+    import torch
+    import compact_schemes_b200 as cs
+    R = ctypes.CDLL(REF_GPU)
+    vp = ctypes.c_void_p
+    R.ref_gpu_fluxes_pre.argtypes = [vp] * 9 + [ctypes.c_double] * 3 + [ctypes.c_uint, vp, vp]
+    dims = (64, 64, 64)
+    n = int(np.prod(dims))
+    rng = np.random.default_rng(7)
+    xim, etm, zem, _ = metric_fields(dims)
+    rho = 1.0 + 0.1 * rng.random(n)
+    vel = 0.3 * rng.standard_normal((3, n))
+    p = 1 / 1.4 + 0.05 * rng.random(n)
+    qa = np.concatenate([rho, rho * vel[0], rho * vel[1], rho * vel[2], p / 0.4 + 0.5 * rho * (vel ** 2).sum(0)])
+    de = np.concatenate([1 / rho, vel[0], vel[1], vel[2], 1.4 * p / rho])
+    tau = 1e-3 * rng.standard_normal(6 * n)
+    heat = 1e-3 * rng.standard_normal(3 * n)
+    umf = (0.05, -0.02, 0.01)
+    ph = cs.physics(dims, True)
+    ph.umf = umf
+    b0, _, dtau, dheat = ph.buffers()
+    device_view(dtau, 6 * n).copy_(dev(tau))
+    device_view(dheat, 3 * n).copy_(dev(heat))
+    d_de = dev(de)
+    args = [dev(a) for a in (qa, p, xim, etm, zem)]
+    ph.calc_fluxes_pre(args[0], args[1], d_de, args[2], args[3], args[4])
+    torch.cuda.synchronize()
+    ours = device_view(b0, 15 * n).cpu().numpy().reshape(15, n)
+    ours_de4 = d_de.cpu().numpy()[4 * n:]
+    theirs = torch.zeros(15 * n, dtype=torch.float64, device=cuda)
+    r_de = dev(de)
+    structs = torch.zeros(16, dtype=torch.float64, device=cuda)
+    rc = R.ref_gpu_fluxes_pre(vp(theirs.data_ptr()), vp(args[0].data_ptr()), vp(args[1].data_ptr()),
+                              vp(r_de.data_ptr()), vp(args[2].data_ptr()), vp(args[3].data_ptr()),
+                              vp(args[4].data_ptr()), vp(dev(tau).data_ptr()), vp(dev(heat).data_ptr()),
+                              *umf, n, vp(structs.data_ptr()), vp(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    th = theirs.cpu().numpy().reshape(15, n)
+    for c in range(15):
+        assert rel(ours[c], th[c]) < 1e-12, c
+    assert rel(ours_de4, r_de.cpu().numpy()[4 * n:]) < 1e-12
