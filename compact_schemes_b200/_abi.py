@@ -99,6 +99,8 @@ def declare(L):
         getattr(L, name).restype = i32
     L.cs_solver_autotune.argtypes = [vp, vp, i32, ctypes.POINTER(ctypes.c_int * 3 * 2), vp]
     L.cs_solver_autotune.restype = i32
+    L.cs_solver_schedule.argtypes = [vp, ctypes.POINTER(ctypes.c_int * 3 * 2)]
+    L.cs_solver_schedule.restype = i32
     L.cs_solver_set_metrics.argtypes = [vp, vp, vp, vp, vp]
     L.cs_solver_set_metrics.restype = i32
     L.cs_grid_metrics.argtypes = [vp, vp, ctypes.POINTER(f64 * 3 * 3), vp, vp, vp, vp, vp]

@@ -153,7 +153,10 @@ struct cs_solver {
     int64_t F[3] = {0, 0, 0};
     int tile[2][3] = {{8, 8, 8}, {8, 8, 16}};  // lines per tile: [gradient|flux][axis]
     int pl[2][3] = {{0, 0, 0}, {0, 0, 0}};     // pipelined kernels per [gradient|flux][axis]
-    int can[2][3] = {{0, 0, 0}, {0, 0, 0}};    // feasible schedules: 1 tile 8, 2 tile 16, 4 pipelined
+    int can[2][3] = {{0, 0, 0}, {0, 0, 0}};    // feasible schedules: 1 tile 8, 2 tile 16, 4 pipelined,
+                                               // 8 TMA-staged (gradient passes)
+    int tma[3] = {0, 0, 0};                    // gradient pass along each axis stages its pencils by TMA
+    int *err = nullptr;                        // device word: nonzero if a TMA staging copy timed out
     int nsm = 0;
     // optional per-pass event timing (eager path only)
     bool profiling = false;
@@ -253,6 +256,12 @@ static PassArgs pass_args(cs_solver *s, int a, int kind) {
 static int grad_pass(cs_solver *s, int a, const double *q, bool dtred, cudaStream_t st) {
     PassTimer pt(s, st, kPassGradX + a);
     const PassArgs p = pass_args(s, a, 0);
+    // the TMA form reads the uniform-grid constants and needs a 16-byte aligned state
+    if (s->tma[a] && !(dtred && s->fm.xim) && reinterpret_cast<uintptr_t>(q) % 16 == 0) {
+        if (a == 0) return launch_grad_tma<0>(p, s->d, q, dtred, s->err, st);
+        if (a == 1) return launch_grad_tma<1>(p, s->d, q, dtred, s->err, st);
+        return launch_grad_tma<2>(p, s->d, q, dtred, s->err, st);
+    }
     if (a == 0) return launch_grad<0>(p, q, dtred, st);
     if (a == 1) return launch_grad<1>(p, q, dtred, st);
     return launch_grad<2>(p, q, dtred, st);
@@ -440,7 +449,7 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         delete s;
         return set_error(CS_ERR_INVALID, "refine %d", cfg->refine);
     }
-    if (cfg->schedule < CS_SCHED_AUTO || cfg->schedule > CS_SCHED_PIPELINE) {
+    if (cfg->schedule < CS_SCHED_AUTO || cfg->schedule > CS_SCHED_TMA) {
         delete s;
         return set_error(CS_ERR_INVALID, "schedule %d", cfg->schedule);
     }
@@ -483,7 +492,13 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
             s->can[k][a] = (bytes(8) <= (size_t)smem_max ? 1 : 0) |
                            (a > 0 && !(elem == 4 && a == 1) && bytes(16) <= (size_t)smem_max ? 2 : 0) |
                            (pl_fits ? 4 : 0);
-            if (!s->pl[k][a] && bytes(s->tile[k][a]) > (size_t)smem_max) {
+            if (k == 0 && cfg->precision == CS_PREC_FP64) {
+                TmaGeom g;
+                size_t tb = 0;
+                if (tma_grad_geometry(a, s->d, s->tab[a]->lt, smem_max, g, tb)) s->can[0][a] |= 8;
+                s->tma[a] = cfg->schedule == CS_SCHED_TMA && (s->can[0][a] & 8);
+            }
+            if (!s->pl[k][a] && !(k == 0 && s->tma[a]) && bytes(s->tile[k][a]) > (size_t)smem_max) {
                 delete s;
                 return set_error(CS_ERR_UNSUPPORTED,
                                  "axis %d: lines of %d points do not fit the fused %s passes (%zu bytes of shared "
@@ -499,7 +514,8 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
               cudaMalloc(&s->rhs, 5 * lmx * sizeof(double)) == cudaSuccess &&
               cudaMalloc(&s->drva, 10 * s->F[0] * sizeof(double)) == cudaSuccess &&
               cudaMalloc(&s->dtacc, 2 * sizeof(unsigned long long)) == cudaSuccess &&
-              cudaMalloc(&s->dt_dev, sizeof(double)) == cudaSuccess;
+              cudaMalloc(&s->dt_dev, sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&s->err, sizeof(int)) == cudaSuccess;
     if (!ok) {
         cs_solver_destroy(s);
         return set_error(CS_ERR_ALLOC, "solver scratch allocation failed");
@@ -518,6 +534,7 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
     }
     cudaMemset(s->dtacc, 0, 2 * sizeof(unsigned long long));
     cudaMemset(s->dt_dev, 0, sizeof(double));
+    cudaMemset(s->err, 0, sizeof(int));
     *out = s;
     return CS_OK;
 }
@@ -556,8 +573,9 @@ int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3]
     const int saved_tile[2][3] = {{s->tile[0][0], s->tile[0][1], s->tile[0][2]},
                                   {s->tile[1][0], s->tile[1][1], s->tile[1][2]}};
     const int saved_pl[2][3] = {{s->pl[0][0], s->pl[0][1], s->pl[0][2]}, {s->pl[1][0], s->pl[1][1], s->pl[1][2]}};
+    const int saved_tma[3] = {s->tma[0], s->tma[1], s->tma[2]};
     if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
-    // candidates, applied to every pass where feasible: tile 8, tile 16, pipelined
+    // candidates, applied to every pass where feasible: tile 8, tile 16, pipelined, TMA-staged (gradients)
     double best[2][3];
     int pick[2][3];
     for (int k = 0; k < 2; ++k)
@@ -569,15 +587,17 @@ int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3]
         CSB_CUDA(cudaStreamSynchronize(st));
         cs_solver_last_dt(s, &dt);
     }
-    // per-point metrics run the one-phase kernels only
-    const int allowed = s->fm.xim ? 3 : 7;
-    for (int c = 0; c < 3 && rc == CS_OK && dt > 0.0; ++c) {
+    // per-point metrics run the one-phase kernels, or the TMA gradient passes
+    // (the metric-reading CFL reduction of the first then stays one-phase)
+    const int allowed = s->fm.xim ? 11 : 15;
+    for (int c = 0; c < 4 && rc == CS_OK && dt > 0.0; ++c) {
         const int bit = 1 << c;
         if (!(allowed & bit)) continue;
         for (int k = 0; k < 2; ++k)
             for (int a = 0; a < 3; ++a) {
                 const bool ok = (s->can[k][a] & bit) != 0;
                 s->pl[k][a] = ok && c == 2;
+                if (k == 0) s->tma[a] = ok && c == 3;
                 s->tile[k][a] = ok && c == 1 ? 16 : 8;
                 if (!(s->can[k][a] & 1) && !s->pl[k][a]) s->tile[k][a] = saved_tile[k][a];
             }
@@ -592,21 +612,34 @@ int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3]
                 const int kind = (k == 0 ? kPassGradX : kPassFluxX) + a;
                 if (!(s->can[k][a] & bit) || !n[kind]) continue;
                 const double t = ms[kind] / n[kind];
-                if (t < best[k][a]) { best[k][a] = t; pick[k][a] = c == 2 ? 0 : (c == 1 ? 16 : 8); }
+                if (t < best[k][a]) { best[k][a] = t; pick[k][a] = c == 3 ? 1 : (c == 2 ? 0 : (c == 1 ? 16 : 8)); }
             }
     }
     cudaFree(scratch);
     if (rc || !(dt > 0.0)) {
         for (int k = 0; k < 2; ++k)
-            for (int a = 0; a < 3; ++a) { s->tile[k][a] = saved_tile[k][a]; s->pl[k][a] = saved_pl[k][a]; }
+            for (int a = 0; a < 3; ++a) {
+                s->tile[k][a] = saved_tile[k][a];
+                s->pl[k][a] = saved_pl[k][a];
+                if (k == 0) s->tma[a] = saved_tma[a];
+            }
         return rc ? rc : set_error(CS_ERR_STATE, "autotune: no time step from the state");
     }
     for (int k = 0; k < 2; ++k)
         for (int a = 0; a < 3; ++a) {
             s->pl[k][a] = pick[k][a] == 0;
-            s->tile[k][a] = pick[k][a] == 0 ? 8 : pick[k][a];
+            if (k == 0) s->tma[a] = pick[k][a] == 1;
+            s->tile[k][a] = pick[k][a] <= 1 ? 8 : pick[k][a];
             if (choice) choice[k][a] = pick[k][a];
         }
+    return CS_OK;
+}
+
+int cs_solver_schedule(const cs_solver *s, int choice[2][3]) {
+    if (!s || !choice) return set_error(CS_ERR_INVALID, "null argument");
+    for (int k = 0; k < 2; ++k)
+        for (int a = 0; a < 3; ++a)
+            choice[k][a] = s->pl[k][a] ? 0 : (k == 0 && s->tma[a] ? 1 : s->tile[k][a]);
     return CS_OK;
 }
 
@@ -639,7 +672,7 @@ int cs_solver_destroy(cs_solver *s) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
     for (void *p : {(void *)s->q1, (void *)s->grad, (void *)s->rhs, (void *)s->drva, (void *)s->dtacc,
                     (void *)s->dt_dev, (void *)s->qhost_dev, (void *)s->sh32, (void *)s->grad32,
-                    (void *)s->rhs32})
+                    (void *)s->rhs32, (void *)s->err})
         if (p) cudaFree(p);
     delete s;
     return CS_OK;
@@ -724,6 +757,9 @@ int cs_solver_step_host(cs_solver *s, const double *q_in_host, double *q_out_hos
 int cs_solver_last_dt(cs_solver *s, double *dt) {
     if (!s || !dt) return set_error(CS_ERR_INVALID, "null argument");
     CSB_CUDA(cudaMemcpy(dt, s->dt_dev, sizeof(double), cudaMemcpyDeviceToHost));
+    int e = 0;
+    CSB_CUDA(cudaMemcpy(&e, s->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return set_error(CS_ERR_TIMEOUT, "a TMA staging copy of a gradient pass did not complete (code %#x)", e);
     return CS_OK;
 }
 

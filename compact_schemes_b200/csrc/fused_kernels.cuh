@@ -488,6 +488,24 @@ int launch_flux_tl(const PassArgs &a, int mode, const double *q, const double *q
     }
 }
 
+// Geometry of the TMA copies of one gradient-pass tile (tma_grad.cuh).
+struct TmaGeom {
+    int nbox;     // copies along the line (1 or 2)
+    int boxlen;   // points per copy along the line
+    int ntiles;   // tiles of the pass
+    int tiles_x;  // y axis: tiles per x row; unused otherwise
+    unsigned tile_bytes;  // bytes of one staged tile (all copies, OOB fill included)
+};
+// Copy geometry of a TMA gradient pass along `axis`; false when that form
+// does not apply (lines longer than 512 points, row strides that are not
+// multiples of 16 bytes, or more shared memory than smem_max).
+bool tma_grad_geometry(int axis, const cs_dcomp &d, int lt, int smem_max, TmaGeom &g, size_t &smem_bytes);
+// TMA-staged gradient pass along AXIS (tma_grad_axis{0,1,2}.cu); err receives
+// a nonzero code if a staging copy did not complete in time.
+template <int AXIS>
+int launch_grad_tma(const PassArgs &a, const cs_dcomp &d, const double *q, bool dtred, int *err,
+                    cudaStream_t st);
+
 // Per-axis entry points (fused_axis{0,1,2}.cu); they run the pipelined
 // kernels (pipeline_axis{0,1,2}.cu) when PassArgs::pl is set.
 template <int AXIS>

@@ -1,0 +1,298 @@
+// tma_grad.cuh -- gradient pass with pencils staged into shared memory by TMA.
+//
+// Persistent CTAs (one per SM, 16 warps) walk the tiles t_k = blockIdx.x +
+// k * gridDim.x of a gradient pass.  A tile is TL lines of the state q along
+// AXIS; one thread issues it as tensor copies (cp.async.bulk.tensor, no
+// multicast) of all five conserved fields into one of two staging buffers,
+// completing on that buffer's mbarrier, two tiles ahead of the tile being
+// solved.  The y and z pencils are boxes of TL consecutive x (or x-y)
+// positions by the whole line, so the strided lines arrive as dense rows of
+// 64 bytes; the x pencils are TL consecutive rows.  Per tile:
+//   1. wait for the staging buffer (bounded);
+//   2. every thread reads its points of the staged q, forms the primitives
+//      (u, v, w, T) and writes them into the line-solver layout (the staged
+//      rows are read along the tile's x, the transposition into lines happens
+//      here), and reduces the CFL maxima when asked;
+//   3. one thread refills the staging buffer with tile k + 2;
+//   4. warp w solves fields 2 (w / TL) .. +1 (TL = 8) or field w / TL
+//      (TL = 4) of line w % TL in place;
+//   5. the four derivatives go to HBM with coalesced stores.
+// So the HBM reads of two tiles are in flight while a tile is formed, solved
+// and stored, with no per-element address arithmetic on the load side.  The
+// arithmetic is that of k_grad (same primitives, same right-hand sides, same
+// warp solves and field grouping): results are bit-identical to it.
+//
+// Lines of up to 256 points are one box; up to 512 points, two boxes along
+// the line (a TMA box dimension holds at most 256 elements).  Boxes that
+// reach past the end of the array read zeros (TMA out-of-bounds fill); those
+// lines are never stored and their CFL terms are skipped.
+#pragma once
+
+#include <cuda.h>
+
+#include "pipeline.cuh"
+
+namespace csb {
+
+constexpr int kTmaThreads = 512;
+constexpr int kTmaWarps = kTmaThreads / 32;
+// iterations of a bounded mbarrier wait (each try_wait suspends for a
+// hardware-chosen time; with the backoff below the limit is well over 1 s)
+constexpr unsigned kTmaWaitLimit = 1u << 22;
+constexpr int kErrTmaTimeout = 0x7101;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase `parity` of a barrier; false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
+    for (unsigned it = 0; it < kTmaWaitLimit; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it > 8) __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Lines per tile of the TMA gradient pass for chunk length LT.
+template <int LT>
+constexpr int tma_tile() {
+    return LT <= 8 ? 8 : 4;
+}
+
+// Staged offset of field f, tile line l, line point j (box b = j / boxlen).
+template <int AXIS, int TL>
+__device__ __forceinline__ int tma_staged(int f, int l, int j, const TmaGeom &g) {
+    int b = 0, jj = j;
+    while (jj >= g.boxlen) {
+        jj -= g.boxlen;
+        ++b;
+    }
+    const int box = b * 5 * TL * g.boxlen;
+    if (AXIS == 0) return box + (f * TL + l) * g.boxlen + jj;
+    return box + (f * g.boxlen + jj) * TL + l;
+}
+
+// Issue the copies of tile t into the staging buffer dst (one thread).
+template <int AXIS, int TL>
+__device__ __forceinline__ void tma_issue_tile(double *dst, const CUtensorMap *map, int t, const TmaGeom &g,
+                                               uint64_t *bar) {
+    mbar_arrive_expect_tx(bar, g.tile_bytes);
+    for (int b = 0; b < g.nbox; ++b) {
+        double *d = dst + b * 5 * TL * g.boxlen;
+        if (AXIS == 0) tma_load_3d(d, map, b * g.boxlen, t * TL, 0, bar);
+        else if (AXIS == 1) tma_load_4d(d, map, (t % g.tiles_x) * TL, b * g.boxlen, t / g.tiles_x, 0, bar);
+        else tma_load_3d(d, map, t * TL, b * g.boxlen, 0, bar);
+    }
+}
+
+// Linear index of point j of tile line l, and whether the line exists.
+template <int AXIS, int TL>
+__device__ __forceinline__ bool tma_line(int t, int l, const TmaGeom &g, int lxi, int let, int64_t F,
+                                         int64_t &base, int64_t &stride) {
+    if (AXIS == 0) {
+        const int64_t fidx = (int64_t)t * TL + l;
+        base = fidx * lxi;
+        stride = 1;
+        return fidx < F;
+    }
+    if (AXIS == 1) {
+        const int i = (t % g.tiles_x) * TL + l, k = t / g.tiles_x;
+        base = i + (int64_t)lxi * let * k;
+        stride = lxi;
+        return i < lxi;
+    }
+    const int64_t fidx = (int64_t)t * TL + l;
+    base = fidx;
+    stride = (int64_t)lxi * let;
+    return fidx < F;
+}
+
+// Points (l, j) of a tile owned by this thread: x tiles give each line
+// kTmaWarps / TL warps walking it with lane-consecutive j; y/z tiles give
+// thread t line t % TL and rows t / TL + (kTmaThreads / TL) k.
+template <int AXIS, int TL, typename Fn>
+__device__ __forceinline__ void tma_points(int n, Fn &&fn) {
+    const int tid = threadIdx.x;
+    if (AXIS == 0) {
+        constexpr int WPL = kTmaWarps / TL;
+        const int w = tid >> 5, l = w % TL;
+        for (int j = (w / TL) * 32 + (tid & 31); j < n; j += 32 * WPL) fn(l, j);
+    } else {
+        const int l = tid % TL;
+        for (int j = tid / TL; j < n; j += kTmaThreads / TL) fn(l, j);
+    }
+}
+
+template <int LT, int AXIS, bool DTRED>
+__global__ void __launch_bounds__(kTmaThreads, 1)
+k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, DevTables<double> tab, TmaGeom geo,
+           int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf, Phys ph,
+           unsigned long long *__restrict__ dtacc, int *__restrict__ err) {
+    constexpr int TL = tma_tile<LT>();
+    constexpr int FPW = 4 * TL / kTmaWarps;  // fields per warp solve
+    using L = LineLayout<LT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int stage_elems = geo.nbox * 5 * TL * geo.boxlen;
+    // staging boxes start on 1024-byte boundaries (the launch adds the slack)
+    double *stage0 = reinterpret_cast<double *>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
+    double *solve = stage0 + 2 * stage_elems;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(solve + 4 * TL * L::kSlot);
+    const int n = tab.n;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    const int G = gridDim.x;
+    const int K = geo.ntiles > (int)blockIdx.x ? (geo.ntiles - 1 - (int)blockIdx.x) / G + 1 : 0;
+    if (tid == 0)
+        for (int k = 0; k < 2 && k < K; ++k)
+            tma_issue_tile<AXIS, TL>(stage0 + k * stage_elems, &qmap, blockIdx.x + k * G, geo, &bars[k]);
+    double m1 = 0.0, m2 = 0.0;
+    for (int k = 0; k < K; ++k) {
+        const int t = blockIdx.x + k * G, b = k & 1;
+        double *stg = stage0 + b * stage_elems;
+        const bool ok = mbar_wait_bounded(&bars[b], (unsigned)(k >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            // a copy never completed: record it, let the other buffer's copy
+            // (if any) land within the same limit, and leave
+            if (tid == 0) {
+                atomicExch(err, kErrTmaTimeout);
+                if (k + 1 < K) (void)mbar_wait_bounded(&bars[b ^ 1], (unsigned)((k + 1) >> 1) & 1u);
+            }
+            return;
+        }
+        // primitives into the line layout
+        tma_points<AXIS, TL>(n, [&](int l, int j) {
+            int64_t base, stride;
+            if (!tma_line<AXIS, TL>(t, l, geo, lxi, let, F, base, stride)) return;
+            const Prim s = primitives(stg[tma_staged<AXIS, TL>(0, l, j, geo)], stg[tma_staged<AXIS, TL>(1, l, j, geo)],
+                                      stg[tma_staged<AXIS, TL>(2, l, j, geo)], stg[tma_staged<AXIS, TL>(3, l, j, geo)],
+                                      stg[tma_staged<AXIS, TL>(4, l, j, geo)]);
+            const int pj = L::pos(j);
+            field_line<LT, TL>(solve, 0, l)[pj] = s.u;
+            field_line<LT, TL>(solve, 1, l)[pj] = s.v;
+            field_line<LT, TL>(solve, 2, l)[pj] = s.w;
+            field_line<LT, TL>(solve, 3, l)[pj] = s.T;
+            if (DTRED) {
+                // calc_time_step_kernel (src/cuda/kernels/physics.hpp:335-427), uniform metrics
+                const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
+                double rr2 = 0.0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    rr2 += fabs(xmul(ph.M[a][0], uu) + xmul(ph.M[a][1], vv) + xmul(ph.M[a][2], ww));
+                const double ssi = fabs(ph.J);
+                const double v1 = xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi);
+                const double v2 = s.ri * ph.mu * ph.rr1 * ssi * ssi;
+                m1 = fmax(m1, v1);
+                m2 = fmax(m2, v2);
+            }
+        });
+        __syncthreads();
+        if (tid == 0 && k + 2 < K) tma_issue_tile<AXIS, TL>(stg, &qmap, t + 2 * G, geo, &bars[b]);
+        {
+            int64_t base, stride;
+            const int l = w % TL;
+            if (tma_line<AXIS, TL>(t, l, geo, lxi, let, F, base, stride))
+                solve_group<LT, TL, FPW>(solve, l, (w / TL) * FPW, 4, lane, tab, nstart, nend, cf);
+        }
+        __syncthreads();
+        tma_points<AXIS, TL>(n, [&](int l, int j) {
+            int64_t base, stride;
+            if (!tma_line<AXIS, TL>(t, l, geo, lxi, let, F, base, stride)) return;
+            const int64_t gi = base + j * stride;
+            const int pj = L::pos(j);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) g[c * lmx + gi] = field_line<LT, TL>(solve, c, l)[pj];
+        });
+        __syncthreads();
+    }
+    if (DTRED) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+            m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+        }
+        if (lane == 0) {
+            atomicMax(dtacc, (unsigned long long)__double_as_longlong(m1));
+            atomicMax(dtacc + 1, (unsigned long long)__double_as_longlong(m2));
+        }
+    }
+}
+
+// Host side (tma_grad.cu).
+// Encode the tensor map of q [5][lmx] for a gradient pass along `axis`.
+int tma_grad_map(int axis, const cs_dcomp &d, const TmaGeom &g, const double *q, CUtensorMap &map);
+
+template <int LT, int AXIS>
+int launch_grad_tma_t(const PassArgs &a, const cs_dcomp &d, const double *q, bool dtred, int *err,
+                      cudaStream_t st) {
+    TmaGeom geo;
+    size_t smem = 0;
+    if (!tma_grad_geometry(AXIS, d, LT, 1 << 30, geo, smem))
+        return set_error(CS_ERR_UNSUPPORTED, "TMA gradient pass: unsupported geometry");
+    CUtensorMap map;
+    if (int rc = tma_grad_map(AXIS, d, geo, q, map)) return rc;
+    auto kern = dtred ? k_grad_tma<LT, AXIS, true> : k_grad_tma<LT, AXIS, false>;
+    if (int rc = set_smem(kern, smem)) return rc;
+    const int blocks = geo.ntiles < a.nsm ? geo.ntiles : a.nsm;
+    kern<<<blocks, kTmaThreads, smem, st>>>(map, a.grad + (int64_t)AXIS * 4 * a.lmx, a.tab->t64, geo, a.lxi, a.let,
+                                            a.lmx, a.F, a.nstart, a.nend, a.cf, a.ph, a.dtacc, err);
+    CSB_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+template <int AXIS>
+int launch_grad_tma_impl(const PassArgs &a, const cs_dcomp &d, const double *q, bool dtred, int *err, cudaStream_t st) {
+    switch (a.tab->lt) {
+        case 2: return launch_grad_tma_t<2, AXIS>(a, d, q, dtred, err, st);
+        case 4: return launch_grad_tma_t<4, AXIS>(a, d, q, dtred, err, st);
+        case 8: return launch_grad_tma_t<8, AXIS>(a, d, q, dtred, err, st);
+        case 16: return launch_grad_tma_t<16, AXIS>(a, d, q, dtred, err, st);
+    }
+    return set_error(CS_ERR_UNSUPPORTED, "chunk length");
+}
+
+}  // namespace csb

@@ -30,6 +30,7 @@ REFINE_FLUX = 2  # mixed: refinement in the flux passes only
 SCHED_AUTO = 0
 SCHED_ONEPHASE = 1
 SCHED_PIPELINE = 2
+SCHED_TMA = 3
 
 
 def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, dims=None,
@@ -109,9 +110,17 @@ class Solver:
                                         ctypes.c_void_p(q_out.data_ptr()), float(dt),
                                         stream_ptr(stream)))
 
+    def schedule(self):
+        """Current schedule per pass: {(kind, axis): 8 | 16 (one-phase tile
+        lines) | 0 (pipelined) | 1 (TMA-staged gradient pass)}."""
+        ch = (ctypes.c_int * 3 * 2)()
+        check(lib().cs_solver_schedule(self._h, ctypes.byref(ch)))
+        return {(k, a): ch[k][a] for k in range(2) for a in range(3)}
+
     def autotune(self, q, reps=2, stream=None):
         """Pick the fastest schedule per pass on a scratch copy of q; returns
-        {(kind, axis): 8 | 16 (one-phase tile lines) | 0 (pipelined)}."""
+        {(kind, axis): 8 | 16 (one-phase tile lines) | 0 (pipelined) |
+        1 (TMA-staged gradient pass)}."""
         ch = (ctypes.c_int * 3 * 2)()
         check(lib().cs_solver_autotune(self._h, ptr(q), int(reps), ctypes.byref(ch), stream_ptr(stream)))
         return {(k, a): ch[k][a] for k in range(2) for a in range(3)}
@@ -137,7 +146,7 @@ def tgv_init(q, dims, mach=0.1, noise=1e-4, seed=0, stream=None):
 
 
 def _main(argv=None):
-    """python -m compact_schemes_b200.solver --n N [--precision P] [--steps K] [--curvilinear A]:
+    """python -m compact_schemes_b200.solver --n N [--precision P] [--steps K] [--curvilinear A] [--schedule S]:
     K CFL-stepped RK steps of the N^3 Taylor-Green box (profiling driver);
     with A > 0 on the periodic wavy grid x = xi + A sin(eta) sin(zeta)
     (and cyclic), metrics read per point."""
@@ -149,9 +158,10 @@ def _main(argv=None):
     p.add_argument("--steps", type=int, default=1)
     p.add_argument("--graph", type=int, default=0)
     p.add_argument("--curvilinear", type=float, default=0.0)
+    p.add_argument("--schedule", type=int, default=SCHED_AUTO)
     a = p.parse_args(argv)
     from compact_schemes_b200 import solver as S  # the package's classes, not __main__'s
-    s = S.Solver(S.tgv_config(a.n, precision=a.precision, use_graph=bool(a.graph)))
+    s = S.Solver(S.tgv_config(a.n, precision=a.precision, use_graph=bool(a.graph), schedule=a.schedule))
     if a.curvilinear > 0:
         import compact_schemes_b200 as cs
         n = a.n

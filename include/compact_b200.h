@@ -250,6 +250,10 @@ typedef struct cs_solver cs_solver;
 #define CS_SCHED_ONEPHASE 1 /* each CTA loads a tile, solves it, stores it (tile[][] applies) */
 #define CS_SCHED_PIPELINE 2 /* persistent CTAs: memory warps store tile k-1 and stage tile k+1
                                while solver warps solve tile k; error where the tiles do not fit */
+#define CS_SCHED_TMA 3      /* gradient passes: persistent CTAs whose pencils of the state are
+                               staged into shared memory by TMA two tiles ahead (FP64, lines of
+                               up to 512 points, even row lengths; else one-phase); flux passes
+                               one-phase */
 
 typedef struct {
     int lxi, let, lze;  /* points per axis */
@@ -300,9 +304,12 @@ int cs_solver_dt_device(cs_solver *s, double **dt_dev);
 /* Autotuner: times `reps` eager steps of every feasible pass schedule (one-
  * phase with 8- or 16-line tiles, pipelined) on a scratch copy of q (q is not
  * modified) and keeps the fastest per pass; choice[kind][axis] (may be NULL)
- * receives 8 or 16 (one-phase tile lines) or 0 (pipelined) for the gradient
- * (kind 0) and flux (kind 1) passes.  Synchronizes. */
+ * receives 8 or 16 (one-phase tile lines), 0 (pipelined) or 1 (TMA-staged,
+ * gradient passes) for the gradient (kind 0) and flux (kind 1) passes.
+ * Synchronizes. */
 int cs_solver_autotune(cs_solver *s, const double *q, int reps, int choice[2][3], void *stream);
+/* The schedule each pass runs now, coded as cs_solver_autotune's choice. */
+int cs_solver_schedule(const cs_solver *s, int choice[2][3]);
 /* Per-point metrics for the fused solver: device arrays xim, etm, zem
  * ([3][lmx], J^-1 grad(xi_a)) and yaco ([lmx], J), as cs_grid_metrics
  * writes them, read by every later step, stage and RHS call instead of the
