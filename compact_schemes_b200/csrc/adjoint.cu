@@ -261,6 +261,8 @@ int cs_adjoint_create(cs_adjoint **out, const cs_solver_config *cfg) {
     if (!out || !cfg) return set_error(CS_ERR_INVALID, "null argument");
     *out = nullptr;
     if (cfg->precision != CS_PREC_FP64) return set_error(CS_ERR_UNSUPPORTED, "adjoint: FP64 only");
+    if (cfg->filter != CS_FILTER_NONE)
+        return set_error(CS_ERR_UNSUPPORTED, "adjoint: the step map has no filter (cs_adjoint_filter applies it)");
     auto *a = new cs_adjoint();
     a->cfg = *cfg;
     a->cfg.use_graph = 0;  // the stages run with per-step time steps

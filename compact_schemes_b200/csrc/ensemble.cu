@@ -208,6 +208,7 @@ int cs_ensemble_create(cs_ensemble **out, int nbox, const cs_solver_config *boxe
         if ((c.viscous != 0) != e->viscous) return fail(CS_ERR_UNSUPPORTED, "all boxes viscous or all inviscid");
         if (c.precision != CS_PREC_FP64) return fail(CS_ERR_UNSUPPORTED, "FP64 only");
         if (c.gcbc) return fail(CS_ERR_UNSUPPORTED, "no characteristic boundary closure");
+        if (c.filter != CS_FILTER_NONE) return fail(CS_ERR_UNSUPPORTED, "no filter in the ensemble step");
         if (!(c.dx > 0 && c.dy > 0 && c.dz > 0)) return fail(CS_ERR_INVALID, "grid spacing");
         const int n[3] = {c.lxi, c.let, c.lze};
         bx.lxi = c.lxi;

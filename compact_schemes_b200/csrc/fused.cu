@@ -157,6 +157,7 @@ struct cs_solver {
                                                // 8 TMA-staged (gradient passes)
     int tma[3] = {0, 0, 0};                    // gradient pass along each axis stages its pencils by TMA
     int *err = nullptr;                        // device word: nonzero if a TMA staging copy timed out
+    const DeviceTables *ftab[3] = {nullptr, nullptr, nullptr};  // filter tables (cfg.filter)
     int nsm = 0;
     // optional per-pass event timing (eager path only)
     bool profiling = false;
@@ -173,7 +174,8 @@ namespace csb {
 
 // Pass kinds reported by cs_solver_profile_end.
 enum PassKind { kPassGradX = 0, kPassGradY, kPassGradZ, kPassFluxX, kPassFluxY, kPassFluxZ, kPassGcbc,
-                kPassKinds };
+                kPassFilter, kPassKinds };
+static_assert(kPassKinds == CS_PASS_KINDS, "pass kinds");
 
 static cudaEvent_t take_event(cs_solver *s) {
     if (!s->event_pool.empty()) {
@@ -386,6 +388,16 @@ static int run_stage_mx(cs_solver *s, const double *qin, const double *qn, doubl
     return CS_OK;
 }
 
+// The compact filter over every active axis, in place on the state q.
+static int filter_pass(cs_solver *s, double *q, cudaStream_t st) {
+    for (int a = 0; a < 3; ++a) {
+        if (!s->active[a]) continue;
+        PassTimer pt(s, st, kPassFilter);
+        if (int rc = filter_state(q, a, *s->ftab[a], s->d, s->cfg.alpha_f, st)) return rc;
+    }
+    return CS_OK;
+}
+
 static int run_step(cs_solver *s, double *q, double dt, cudaStream_t st) {
     const bool cfl = !(dt > 0.0);
     if (cfl) CSB_CUDA(cudaMemsetAsync(s->dtacc, 0, 2 * sizeof(unsigned long long), st));
@@ -400,10 +412,16 @@ static int run_step(cs_solver *s, double *q, double dt, cudaStream_t st) {
         double *qout = k == 3 ? q : s->q1;
         if (s->mixed) {
             if (int rc = run_stage_mx(s, qin, q, qout, false, &rk, k == 0, k < 3, st)) return rc;
+            if (k == 3 && s->cfg.filter == CS_FILTER_STEP)
+                if (int rc = filter_pass(s, q, st)) return rc;
             continue;
         }
         if (int rc = run_stage(s, qin, q, qout, nullptr, &rk, cfl && k == 0, st)) return rc;
+        if (s->cfg.filter == CS_FILTER_STAGE)
+            if (int rc = filter_pass(s, qout, st)) return rc;
     }
+    if (s->cfg.filter == CS_FILTER_STEP)
+        if (int rc = filter_pass(s, q, st)) return rc;
     return CS_OK;
 }
 
@@ -448,6 +466,29 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
     if (cfg->refine < CS_REFINE_NONE || cfg->refine > CS_REFINE_FLUX) {
         delete s;
         return set_error(CS_ERR_INVALID, "refine %d", cfg->refine);
+    }
+    if (cfg->filter < CS_FILTER_NONE || cfg->filter > CS_FILTER_STAGE) {
+        delete s;
+        return set_error(CS_ERR_INVALID, "filter %d", cfg->filter);
+    }
+    if (cfg->filter != CS_FILTER_NONE) {
+        if (!(cfg->alpha_f > -0.5 && cfg->alpha_f <= 0.5)) {
+            delete s;
+            return set_error(CS_ERR_INVALID, "alpha_f %g: the filter needs -0.5 < alpha_f <= 0.5", cfg->alpha_f);
+        }
+        if (cfg->filter == CS_FILTER_STAGE && cfg->precision == CS_PREC_MIXED) {
+            delete s;
+            return set_error(CS_ERR_UNSUPPORTED, "the mixed form filters after every step only");
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (!s->active[a]) continue;
+            if (llen(s->d, a) < 7) { delete s; return set_error(CS_ERR_UNSUPPORTED, "axis %d: the filter needs 7 points", a); }
+            s->ftab[a] = s->tables.get(llen(s->d, a), kFilter, s->ndf[0][a], s->ndf[1][a], cfg->alpha_f);
+            if (!s->ftab[a] || s->ftab[a]->lt > 16) {
+                delete s;
+                return set_error(CS_ERR_UNSUPPORTED, "axis %d: no filter tables for this line", a);
+            }
+        }
     }
     if (cfg->schedule < CS_SCHED_AUTO || cfg->schedule > CS_SCHED_TMA) {
         delete s;

@@ -488,6 +488,10 @@ int launch_flux_tl(const PassArgs &a, int mode, const double *q, const double *q
     }
 }
 
+// The compact filter along `axis` applied in place to the five conserved
+// fields of q [5][lmx] (filter_pass.cu; kFilter tables of that axis).
+int filter_state(double *q, int axis, const DeviceTables &t, const cs_dcomp &d, double af, cudaStream_t st);
+
 // Geometry of the TMA copies of one gradient-pass tile (tma_grad.cuh).
 struct TmaGeom {
     int nbox;     // copies along the line (1 or 2)

@@ -19,7 +19,8 @@ class SolverConfig(ctypes.Structure):
                 ("umf", ctypes.c_double * 3), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
                 ("dz", ctypes.c_double), ("cfl", ctypes.c_double), ("gcbc", ctypes.c_int),
                 ("use_graph", ctypes.c_int), ("tile", ctypes.c_int * 3 * 2),
-                ("precision", ctypes.c_int), ("refine", ctypes.c_int), ("schedule", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("refine", ctypes.c_int), ("schedule", ctypes.c_int),
+                ("filter", ctypes.c_int), ("alpha_f", ctypes.c_double)]
 
 
 PREC_FP64 = 0
@@ -31,10 +32,14 @@ SCHED_AUTO = 0
 SCHED_ONEPHASE = 1
 SCHED_PIPELINE = 2
 SCHED_TMA = 3
+FILTER_NONE = 0   # no filter in the time step
+FILTER_STEP = 1   # compact filter x, y, z on the state after every RK step
+FILTER_STAGE = 2  # the same after every RK stage (FP64 only)
 
 
 def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, dims=None,
-               nbc=None, gcbc=False, tile=None, precision=PREC_FP64, refine=REFINE_NONE, schedule=SCHED_AUTO):
+               nbc=None, gcbc=False, tile=None, precision=PREC_FP64, refine=REFINE_NONE, schedule=SCHED_AUTO,
+               filter=FILTER_NONE, alpha_f=0.45):
     """Taylor-Green box [0,2pi)^3 in CANARD units: mu = rho0 U0 L / Re with U0 = Mach."""
     lxi, let, lze = dims if dims is not None else (n, n, n)
     c = SolverConfig()
@@ -54,6 +59,8 @@ def tgv_config(n, mach=0.1, re=1600.0, cfl=0.5, viscous=True, use_graph=True, di
     c.precision = int(precision)
     c.refine = int(refine)
     c.schedule = int(schedule)
+    c.filter = int(filter)
+    c.alpha_f = float(alpha_f)
     if tile is not None:
         for k in range(2):
             for a in range(3):
@@ -92,15 +99,15 @@ class Solver:
     def step(self, q, dt=0.0, stream=None):
         check(lib().cs_solver_step(self._h, ptr(q), float(dt), stream_ptr(stream)))
 
-    PASS_NAMES = ("grad_x", "grad_y", "grad_z", "flux_x", "flux_y", "flux_z_rk", "gcbc")
+    PASS_NAMES = ("grad_x", "grad_y", "grad_z", "flux_x", "flux_y", "flux_z_rk", "gcbc", "filter")
 
     def profile_begin(self):
         check(lib().cs_solver_profile_begin(self._h))
 
     def profile_end(self):
         """{pass name: (total ms, launches)} since profile_begin (synchronizes)."""
-        ms = (ctypes.c_double * 7)()
-        n = (ctypes.c_int * 7)()
+        ms = (ctypes.c_double * len(self.PASS_NAMES))()
+        n = (ctypes.c_int * len(self.PASS_NAMES))()
         check(lib().cs_solver_profile_end(self._h, ms, n))
         return {k: (ms[i], n[i]) for i, k in enumerate(self.PASS_NAMES)}
 

@@ -250,6 +250,10 @@ typedef struct cs_solver cs_solver;
 #define CS_SCHED_ONEPHASE 1 /* each CTA loads a tile, solves it, stores it (tile[][] applies) */
 #define CS_SCHED_PIPELINE 2 /* persistent CTAs: memory warps store tile k-1 and stage tile k+1
                                while solver warps solve tile k; error where the tiles do not fit */
+#define CS_FILTER_NONE 0  /* no filter in the time step */
+#define CS_FILTER_STEP 1  /* the compact filter along x, y, z on the state after every RK step */
+#define CS_FILTER_STAGE 2 /* the same after every RK stage (FP64 only) */
+
 #define CS_SCHED_TMA 3      /* gradient passes: persistent CTAs whose pencils of the state are
                                staged into shared memory by TMA two tiles ahead (FP64, lines of
                                up to 512 points, even row lengths; else one-phase); flux passes
@@ -273,6 +277,9 @@ typedef struct {
     int refine;         /* mixed: CS_REFINE_ALL one FP64-residual refinement sweep per line
                            solve, CS_REFINE_NONE none, CS_REFINE_FLUX in the flux passes only */
     int schedule;       /* CS_SCHED_*: how a pass overlaps its line solves with its HBM traffic */
+    int filter;         /* CS_FILTER_*: the compact filter of cs_filter applied to the conserved
+                           state inside the time step (all five fields, x then y then z) */
+    double alpha_f;     /* filter parameter, -0.5 < alpha_f <= 0.5 (cs_filter's) */
 } cs_solver_config;
 
 int cs_solver_create(cs_solver **out, const cs_solver_config *cfg);
@@ -299,8 +306,8 @@ int cs_solver_dt_device(cs_solver *s, double **dt_dev);
  * profiled): between begin and end every pass is bracketed by CUDA events on
  * its stream; end synchronizes and returns the summed milliseconds and launch
  * counts per pass kind: 0-2 gradient x/y/z, 3-5 flux x/y/z (z carries the RK
- * update), 6 GCBC. */
-#define CS_PASS_KINDS 7
+ * update), 6 GCBC, 7 filter (one launch per axis). */
+#define CS_PASS_KINDS 8
 /* Autotuner: times `reps` eager steps of every feasible pass schedule (one-
  * phase with 8- or 16-line tiles, pipelined) on a scratch copy of q (q is not
  * modified) and keeps the fastest per pass; choice[kind][axis] (may be NULL)

@@ -306,3 +306,86 @@ def test_10_steps_128_match_oracle(cuda):
     mmax = max(np.abs(ref[f]).max() for f in (1, 2, 3))
     err[3] = np.abs(got[3] - ref[3]).max() / mmax
     assert max(err.values()) < 1e-10, err
+
+
+def _filter_state_oracle(q, dims, ndf, alpha_f):
+    """The compact filter along x, then y, then z on each conserved field."""
+    lmx = int(np.prod(dims))
+    for m in range(5):
+        f = q[m * lmx:(m + 1) * lmx]
+        for a in range(3):
+            f = O.filt(f, dims, a, ndf[a], ndf[a], alpha_f)
+        q[m * lmx:(m + 1) * lmx] = f
+
+
+@pytest.mark.parametrize("dims,gcbc", [((32, 24, 20), False), ((36, 24, 20), True)])
+def test_filter_every_step_matches_oracle(cuda, dims, gcbc):
+    """Filter in the time step (CS_FILTER_STEP): three CFL-stepped RK steps,
+    each followed by the sixth-order filter (alpha_f 0.45) along x, y and z
+    on all five conserved fields, against the oracle's RK step and filter at
+    1e-12 (rho w, which starts at 0, relative to the largest momentum)."""
+    import torch
+    import compact_schemes_b200 as cs
+    from compact_schemes_b200.solver import FILTER_STEP
+    nbc = [[10, 45, 45], [10, 45, 45]] if gcbc else [[45] * 3, [45] * 3]
+    ndf = [0, 1, 1] if gcbc else [1, 1, 1]
+    s = solver(dims, use_graph=True, nbc=nbc, gcbc=gcbc, filter=FILTER_STEP, alpha_f=0.45)
+    q = O.tgv_init(dims, 0.3 if gcbc else MACH, 1e-4, 3)
+    qd = dev(q)
+    for _ in range(3):
+        s.step(qd, 0.0)
+        dt = O.rk_step(q, MU, O.uniform_metrics(*dims), dims, nbc, cfl=0.5, gcbc=gcbc)
+        _filter_state_oracle(q, dims, ndf, 0.45)
+    torch.cuda.synchronize()
+    assert abs(s.last_dt() - dt) / dt < 1e-13
+    got = qd.cpu().numpy().reshape(5, -1)
+    ref = q.reshape(5, -1)
+    mmax = max(np.abs(ref[f]).max() for f in (1, 2, 3))
+    err = [np.abs(got[f] - ref[f]).max() / (mmax if f == 3 else np.abs(ref[f]).max()) for f in range(5)]
+    assert max(err) < 1e-12, err
+    # the filter changed the state (against an unfiltered step)
+    s2 = solver(dims, use_graph=False, nbc=nbc, gcbc=gcbc)
+    q2 = dev(O.tgv_init(dims, 0.3 if gcbc else MACH, 1e-4, 3))
+    for _ in range(3):
+        s2.step(q2, 0.0)
+    assert float((q2 - qd).abs().max()) > 0.0
+
+
+def test_filter_every_stage_matches_oracle(cuda):
+    """CS_FILTER_STAGE: the filter after each of the four RK stages, fixed dt."""
+    import torch
+    from compact_schemes_b200.solver import FILTER_STAGE
+    dims = (32, 24, 20)
+    nbc = [[45] * 3, [45] * 3]
+    s = solver(dims, use_graph=False, filter=FILTER_STAGE, alpha_f=0.3)
+    q = O.tgv_init(dims, MACH, 1e-4, 4)
+    qd = dev(q)
+    m = O.uniform_metrics(*dims)
+    dt = 0.01
+    for _ in range(2):
+        s.step(qd, dt)
+        qn = q.copy()
+        qs = q.copy()
+        for k in range(4):
+            out = np.empty_like(q)
+            O.rk_stage(qn, qs, out, k, dt, MU, m, dims, nbc)
+            _filter_state_oracle(out, dims, [1, 1, 1], 0.3)
+            qs = out
+        q = qs
+    torch.cuda.synchronize()
+    got = qd.cpu().numpy().reshape(5, -1)
+    ref = q.reshape(5, -1)
+    mmax = max(np.abs(ref[f]).max() for f in (1, 2, 3))
+    err = [np.abs(got[f] - ref[f]).max() / (mmax if f == 3 else np.abs(ref[f]).max()) for f in range(5)]
+    assert max(err) < 1e-12, err
+
+
+def test_filter_config_rejected_where_unsupported(cuda):
+    import compact_schemes_b200 as cs
+    from compact_schemes_b200.solver import FILTER_STAGE, FILTER_STEP
+    with pytest.raises(cs.CSError):
+        solver((32, 24, 20), filter=FILTER_STEP, alpha_f=0.7)
+    with pytest.raises(cs.CSError):
+        solver((32, 24, 20), filter=FILTER_STAGE, precision=1)
+    with pytest.raises(cs.CSError):
+        cs.Adjoint(cs.tgv_config(None, dims=(32, 24, 20), filter=FILTER_STEP))
