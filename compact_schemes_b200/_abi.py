@@ -37,6 +37,8 @@ def declare(L):
     L.cs_calc_viscous_shear_stress.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, Dcomp, vp]
     L.cs_calc_time_step.argtypes = [vp, vp, vp, vp, vp, vp, vp, f64, ctypes.POINTER(f64), sz, vp]
     L.cs_gcbc_go.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, Dcomp, vp, vp]
+    L.cs_gcbc_apply.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, Dcomp, ctypes.c_double, vp, vp, vp]
+    L.cs_gcbc_apply.restype = i32
     L.cs_thermo.argtypes = [vp, vp, vp, sz, vp]
     L.cs_wall_condition_update.argtypes = [vp, vp, ctypes.POINTER(f64), Dcomp, vp, vp]
     L.cs_wall_condition_update.restype = i32

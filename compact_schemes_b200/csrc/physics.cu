@@ -237,6 +237,189 @@ __global__ void k_gcbc_face(double *__restrict__ de, const double *__restrict__ 
     }
 }
 
+// Characteristic state of one face point (gcbc_vgpr::eleme,
+// src/cuda/kernels/gcbc.hpp:43-57) and the two transformation matrices
+// (xtr2q :59-107, xtq2r :109-150 with its typos fixed: dm[2] = aoi c[2],
+// xt[0][4] = -ho c[0], xt[4][0] = 1 - bo + co), in the oracle's operation order.
+struct GcPt {
+    double c[3], ve[3], hv2, ao, aoi, vn, vs;
+};
+__device__ __forceinline__ GcPt gc_eleme(const double c[3], double rho, double m0, double m1, double m2, double pp,
+                                         double u0, double u1, double u2) {
+    GcPt g;
+    const double rhoi = 1.0 / rho;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) g.c[k] = c[k];
+    g.ao = sqrt(xmul(xmul(kGam, rhoi), pp));
+    g.aoi = 1.0 / g.ao;
+    g.ve[0] = xmul(rhoi, m0);
+    g.ve[1] = xmul(rhoi, m1);
+    g.ve[2] = xmul(rhoi, m2);
+    g.hv2 = xmul(0.5, xmul(g.ve[0], g.ve[0]) + xmul(g.ve[1], g.ve[1]) + xmul(g.ve[2], g.ve[2]));
+    g.vn = xmul(c[0], g.ve[0]) + xmul(c[1], g.ve[1]) + xmul(c[2], g.ve[2]);
+    g.vs = xmul(c[0], u0) + xmul(c[1], u1) + xmul(c[2], u2);
+    return g;
+}
+__device__ __forceinline__ void gc_xtq2r(const GcPt &g, double L[5][5]) {
+    const double *c = g.c, *ve = g.ve;
+    const double ho = xmul(xmul(kGamm1, g.aoi), g.aoi), bo = 1.0 - xmul(ho, g.hv2), co = xmul(g.aoi, g.vn);
+    const double dm[3] = {xmul(g.aoi, c[0]), xmul(g.aoi, c[1]), xmul(g.aoi, c[2])};
+    const double rv[3] = {xmul(ho, ve[0]), xmul(ho, ve[1]), xmul(ho, ve[2])};
+    L[0][0] = xmul(bo, c[0]) + xmul(dm[1], ve[2]) - xmul(dm[2], ve[1]);
+    L[0][1] = xmul(c[0], rv[0]);
+    L[0][2] = xmul(c[0], rv[1]) + dm[2];
+    L[0][3] = xmul(c[0], rv[2]) - dm[1];
+    L[0][4] = xmul(-ho, c[0]);
+    L[1][0] = xmul(bo, c[1]) + xmul(dm[2], ve[0]) - xmul(dm[0], ve[2]);
+    L[1][1] = xmul(c[1], rv[0]) - dm[2];
+    L[1][2] = xmul(c[1], rv[1]);
+    L[1][3] = xmul(c[1], rv[2]) + dm[0];
+    L[1][4] = xmul(-ho, c[1]);
+    L[2][0] = xmul(bo, c[2]) + xmul(dm[0], ve[1]) - xmul(dm[1], ve[0]);
+    L[2][1] = xmul(c[2], rv[0]) + dm[1];
+    L[2][2] = xmul(c[2], rv[1]) - dm[0];
+    L[2][3] = xmul(c[2], rv[2]);
+    L[2][4] = xmul(-ho, c[2]);
+    L[3][0] = 1.0 - bo - co;
+    L[3][1] = dm[0] - rv[0];
+    L[3][2] = dm[1] - rv[1];
+    L[3][3] = dm[2] - rv[2];
+    L[3][4] = ho;
+    L[4][0] = 1.0 - bo + co;
+    L[4][1] = -dm[0] - rv[0];
+    L[4][2] = -dm[1] - rv[1];
+    L[4][3] = -dm[2] - rv[2];
+    L[4][4] = ho;
+}
+__device__ __forceinline__ void gc_xtr2q(const GcPt &g, double S[5][5]) {
+    const double *c = g.c, *ve = g.ve;
+    const double bo = g.hv2 + xmul(xmul(kHamm1, g.ao), g.ao), co = xmul(g.ao, g.vn);
+    const double dm[3] = {xmul(g.ao, c[0]), xmul(g.ao, c[1]), xmul(g.ao, c[2])};
+    S[0][0] = c[0];
+    S[0][1] = c[1];
+    S[0][2] = c[2];
+    S[0][3] = 0.5;
+    S[0][4] = 0.5;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+        // row 1 + k: c[j] ve[k] plus the rotation part +-dm[k1], +-dm[k2]
+        S[1 + k][k] = xmul(c[k], ve[k]);
+        S[1 + k][3] = xmul(0.5, ve[k] + dm[k]);
+        S[1 + k][4] = xmul(0.5, ve[k] + dm[k]) - dm[k];
+        S[1 + k][k1] = xmul(c[k1], ve[k]) - dm[k2];
+        S[1 + k][k2] = xmul(c[k2], ve[k]) + dm[k1];
+    }
+    S[4][0] = xmul(g.hv2, c[0]) + xmul(dm[2], ve[1]) - xmul(dm[1], ve[2]);
+    S[4][1] = xmul(g.hv2, c[1]) + xmul(dm[0], ve[2]) - xmul(dm[2], ve[0]);
+    S[4][2] = xmul(g.hv2, c[2]) + xmul(dm[1], ve[0]) - xmul(dm[0], ve[1]);
+    S[4][3] = xmul(0.5, bo + co);
+    S[4][4] = xmul(0.5, bo + co) - co;
+}
+__device__ __forceinline__ void gc_matvec(const double A[5][5], const double *x, double *y) {
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) v += xmul(A[r][k], x[k]);
+        y[r] = v;
+    }
+}
+
+// Face point fi of face ip along AXIS (the derivative's drva face index) and
+// the stride into the block.
+template <int AXIS>
+__device__ __forceinline__ int64_t gc_point(int64_t fi, int ip, int lxi, int let, int lze, int64_t &stride,
+                                            int &dim) {
+    int64_t base;
+    if (AXIS == 0) { base = fi * lxi; stride = 1; dim = lxi; }
+    else if (AXIS == 1) { base = (fi / lxi) * (int64_t)lxi * let + fi % lxi; stride = lxi; dim = let; }
+    else { base = fi; stride = (int64_t)lxi * let; dim = lze; }
+    return base + (int64_t)(ip ? dim - 1 : 0) * stride;
+}
+
+// gcbc_setup_kernel (src/cuda/kernels/gcbc.hpp:251-342): drva of face ip in
+// place into characteristic form, from drva (flag, non-reflective faces) or
+// from the full right-hand side de (walls, curvilinear interfaces), times J.
+template <int AXIS>
+__global__ void k_gc_setup(double *__restrict__ drva, const double *__restrict__ cm, const double *__restrict__ qa,
+                           const double *__restrict__ de, const double *__restrict__ p,
+                           const double *__restrict__ yaco, double u0, double u1, double u2, int ip, int flag,
+                           int lxi, int let, int lze) {
+    const int64_t n = (int64_t)lxi * let * lze;
+    const int64_t F = AXIS == 0 ? (int64_t)let * lze : (AXIS == 1 ? (int64_t)lxi * lze : (int64_t)lxi * let);
+    const int64_t fi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (fi >= F) return;
+    int64_t stride;
+    int dim;
+    const int64_t idx = gc_point<AXIS>(fi, ip, lxi, let, lze, stride, dim);
+    const double c[3] = {cm[(ip * 3 + 0) * F + fi], cm[(ip * 3 + 1) * F + fi], cm[(ip * 3 + 2) * F + fi]};
+    const GcPt g = gc_eleme(c, qa[idx], qa[n + idx], qa[2 * n + idx], qa[3 * n + idx], p[idx], u0, u1, u2);
+    double L[5][5], src[5], cha[5];
+    gc_xtq2r(g, L);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) src[v] = xmul(yaco[idx], flag ? drva[(ip * 5 + v) * F + fi] : de[v * n + idx]);
+    gc_matvec(L, src, cha);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) drva[(ip * 5 + v) * F + fi] = cha[v];
+}
+
+// The update kernels (src/cuda/kernels/gcbc.hpp:344-695) for one face:
+// kind 0 non-reflective (incoming acoustic waves zeroed), 1 wall (incoming
+// acoustic wave reflected from the outgoing one with the frame acceleration
+// and the normal velocity relaxed at rate dtwi), 2 curvilinear interface
+// (incoming waves from the neighbour's drvb).  de += sbcc xtr2q (cha - drva)
+// on kMbci planes; the wall update subtracts drva like the other two (the
+// reference's wall kernel adds xtr2q cha, the whole right-hand side).
+template <int AXIS>
+__global__ void k_gc_update(int kind, const double *__restrict__ drva, const double *__restrict__ drvb,
+                            const double *__restrict__ cm, const double *__restrict__ qa, double *__restrict__ de,
+                            const double *__restrict__ p, const double *__restrict__ sbcc, double u0, double u1,
+                            double u2, double a0, double a1, double a2, double dtwi, int ip, int lxi, int let,
+                            int lze) {
+    const int64_t n = (int64_t)lxi * let * lze;
+    const int64_t F = AXIS == 0 ? (int64_t)let * lze : (AXIS == 1 ? (int64_t)lxi * lze : (int64_t)lxi * let);
+    const int64_t fi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (fi >= F) return;
+    int64_t stride;
+    int dim;
+    const int64_t idx = gc_point<AXIS>(fi, ip, lxi, let, lze, stride, dim);
+    const double c[3] = {cm[(ip * 3 + 0) * F + fi], cm[(ip * 3 + 1) * F + fi], cm[(ip * 3 + 2) * F + fi]};
+    const double rho = qa[idx];
+    const GcPt g = gc_eleme(c, rho, qa[n + idx], qa[2 * n + idx], qa[3 * n + idx], p[idx], u0, u1, u2);
+    double dr[5], cha[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) cha[v] = dr[v] = drva[(ip * 5 + v) * F + fi];
+    const double ra0 = 1.0 - 2.0 * ip;
+    if (kind == 0) {
+        if (ra0 * (g.vn + g.vs + g.ao) > 0) cha[3] = 0.0;
+        if (ra0 * (g.vn + g.vs - g.ao) > 0) cha[4] = 0.0;
+    } else if (kind == 2) {
+        double dh[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) dh[v] = drvb[(ip * 5 + v) * F + fi];
+        if (ra0 * (g.vn + g.vs) > 0) { cha[0] = dh[0]; cha[1] = dh[1]; cha[2] = dh[2]; }
+        if (ra0 * (g.vn + g.vs + g.ao) > 0) cha[3] = dh[3];
+        if (ra0 * (g.vn + g.vs - g.ao) > 0) cha[4] = dh[4];
+    } else {
+        const double acc = xmul(c[0], a0) + xmul(c[1], a1) + xmul(c[2], a2);
+        const double w = xmul(xmul(xmul(2.0, ra0), g.aoi), rho);
+        if (ip == 0) cha[3] = cha[4] + xmul(w, acc + xmul(dtwi, g.vn + g.vs));
+        else cha[4] = cha[3] + xmul(w, acc + xmul(dtwi, g.vn + g.vs));
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) cha[v] -= dr[v];
+    double S[5][5], dq[5];
+    gc_xtr2q(g, S);
+    gc_matvec(S, cha, dq);
+    const int iq = 1 - 2 * ip;
+    for (int ii = 0; ii < kMbci && ii < dim; ++ii) {
+        const int64_t o = idx + (int64_t)ii * iq * stride;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) de[v * n + o] += xmul(sbcc[o], dq[v]);
+    }
+}
+
 // Primitive recovery into the reference's de slots (the empty slot of the
 // driver, driver/canard.cu:142-143): de0 = 1/rho, de1..3 = u, v, w,
 // de4 = gamma p / rho (c^2, the CANARD temperature), p.
@@ -503,7 +686,8 @@ int cs_gcbc_go(cs_numerics *nm, double *const cm[3], const double *qa, double *d
             const int np = nbc[ip][a];
             if (np == CS_BC_PERIODIC || np == CS_BC_INTER_STRAIGHT || np == CS_BC_INTER_SUBDOMAINS) continue;
             if (np != CS_BC_NON_REFLECTIVE)
-                return set_error(CS_ERR_UNSUPPORTED, "gcbc_go: boundary code %d (walls / curvilinear interfaces) is not in this build", np);
+                return set_error(CS_ERR_UNSUPPORTED, "cs_gcbc_go: boundary code %d (walls / curvilinear interfaces) "
+                                 "needs drvb, dudtmf and dtwi: use cs_gcbc_apply", np);
             if (dim < 2) return set_error(CS_ERR_INVALID, "gcbc on a degenerate axis");
             if (!cm[a]) return set_error(CS_ERR_INVALID, "cm[%d] is null", a);
             const unsigned b = blocks_for(F, 128);
@@ -513,6 +697,66 @@ int cs_gcbc_go(cs_numerics *nm, double *const cm[3], const double *qa, double *d
             CSB_CUDA(cudaGetLastError());
         }
     }
+    return CS_OK;
+}
+
+static bool gc_active(int np) {
+    return np == CS_BC_NON_REFLECTIVE || np == CS_BC_WALL_INVISCID || np == CS_BC_WALL_VISCOUS ||
+           np == CS_BC_INTER_CURV;
+}
+
+int cs_gcbc_apply(double *const drva[3], double *const cm[3], double *const drvb[3], const double *qa, double *de,
+                  const double *p, const double *yaco, const double *sbcc, const double umf[3],
+                  const double dudtmf[3], cs_dcomp d, double dtwi, const int nbc[2][3], const int mcd[2][3],
+                  void *stream) {
+    (void)mcd;  // single rank: every curvilinear interface pairs with the block's own opposite face
+    if (!drva || !cm || !drvb || !qa || !de || !p || !yaco || !sbcc || !umf || !dudtmf || !nbc)
+        return set_error(CS_ERR_INVALID, "null argument");
+    if (d.lxi < 1 || d.let < 1 || d.lze < 1 || (int64_t)d.lxi * d.let * d.lze != (int64_t)d.lmx)
+        return set_error(CS_ERR_INVALID, "inconsistent t_dcomp");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int dims[3] = {d.lxi, d.let, d.lze};
+    int64_t F[3] = {(int64_t)d.let * d.lze, (int64_t)d.lxi * d.lze, (int64_t)d.lxi * d.let};
+    for (int a = 0; a < 3; ++a)
+        for (int ip = 0; ip < 2; ++ip) {
+            const int np = nbc[ip][a];
+            if (!gc_active(np)) continue;
+            if (dims[a] < 2) return set_error(CS_ERR_INVALID, "gcbc on a degenerate axis %d", a);
+            if (!drva[a] || !cm[a]) return set_error(CS_ERR_INVALID, "drva[%d] / cm[%d] is null", a, a);
+            if (np == CS_BC_INTER_CURV && !drvb[a]) return set_error(CS_ERR_INVALID, "drvb[%d] is null", a);
+        }
+    // 1. characteristic form of drva (gcbc_setup_kernel)
+    for (int a = 0; a < 3; ++a)
+        for (int ip = 0; ip < 2; ++ip) {
+            const int np = nbc[ip][a];
+            if (!gc_active(np)) continue;
+            const int flag = np == CS_BC_NON_REFLECTIVE;
+            const unsigned b = blocks_for(F[a], 128);
+            if (a == 0) k_gc_setup<0><<<b, 128, 0, st>>>(drva[a], cm[a], qa, de, p, yaco, umf[0], umf[1], umf[2], ip, flag, d.lxi, d.let, d.lze);
+            else if (a == 1) k_gc_setup<1><<<b, 128, 0, st>>>(drva[a], cm[a], qa, de, p, yaco, umf[0], umf[1], umf[2], ip, flag, d.lxi, d.let, d.lze);
+            else k_gc_setup<2><<<b, 128, 0, st>>>(drva[a], cm[a], qa, de, p, yaco, umf[0], umf[1], umf[2], ip, flag, d.lxi, d.let, d.lze);
+            CSB_CUDA(cudaGetLastError());
+        }
+    // 2. GCIC exchange (src/gcbc.hpp:132-157): the neighbour across face ip
+    //    is the block itself, adjacent through its face 1 - ip
+    for (int a = 0; a < 3; ++a)
+        for (int ip = 0; ip < 2; ++ip)
+            if (nbc[ip][a] == CS_BC_INTER_CURV)
+                CSB_CUDA(cudaMemcpyAsync(drvb[a] + (int64_t)ip * 5 * F[a], drva[a] + (int64_t)(1 - ip) * 5 * F[a],
+                                         5 * F[a] * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    // 3. update kernels
+    for (int a = 0; a < 3; ++a)
+        for (int ip = 0; ip < 2; ++ip) {
+            const int np = nbc[ip][a];
+            if (!gc_active(np)) continue;
+            const int kind = np == CS_BC_NON_REFLECTIVE ? 0 : (np == CS_BC_INTER_CURV ? 2 : 1);
+            const unsigned b = blocks_for(F[a], 128);
+            const double *db = drvb[a];
+            if (a == 0) k_gc_update<0><<<b, 128, 0, st>>>(kind, drva[a], db, cm[a], qa, de, p, sbcc, umf[0], umf[1], umf[2], dudtmf[0], dudtmf[1], dudtmf[2], dtwi, ip, d.lxi, d.let, d.lze);
+            else if (a == 1) k_gc_update<1><<<b, 128, 0, st>>>(kind, drva[a], db, cm[a], qa, de, p, sbcc, umf[0], umf[1], umf[2], dudtmf[0], dudtmf[1], dudtmf[2], dtwi, ip, d.lxi, d.let, d.lze);
+            else k_gc_update<2><<<b, 128, 0, st>>>(kind, drva[a], db, cm[a], qa, de, p, sbcc, umf[0], umf[1], umf[2], dudtmf[0], dudtmf[1], dudtmf[2], dtwi, ip, d.lxi, d.let, d.lze);
+            CSB_CUDA(cudaGetLastError());
+        }
     return CS_OK;
 }
 

@@ -101,9 +101,39 @@ def rk_update(qn, de, yaco, dtk, qout, stream=None):
                              stream_ptr(stream)))
 
 
-def gcbc_go(numerics_instance, cm, qa, de, pressure, yaco, sbcc, umf, dcomp, nbc, mcd=None,
-            stream=None):
-    """gcbc_go (src/gcbc.hpp:86-186) for non-reflective faces; drva comes from the numerics object."""
+def gcbc_go(*args, **kw):
+    """gcbc_go (src/gcbc.hpp:86-186).
+
+    Reference signature: gcbc_go(drva_buffer, cm_buffer, drvb_buffer, qa, de,
+    pressure, yaco, sbcc, umf, dudtmf, dcomp_info, dtwi, nbc, mcd) -- every
+    face code (non-reflective, walls, curvilinear interfaces; cs_gcbc_apply);
+    drva_buffer / drvb_buffer / cm_buffer are lists of 3 device pointers or
+    tensors (None where unused).  Also gcbc_go(numerics_instance, cm, qa, de,
+    pressure, yaco, sbcc, umf, dcomp, nbc) for non-reflective faces with drva
+    taken from the numerics object (cs_gcbc_go)."""
+    if hasattr(args[0], "handle"):
+        return _gcbc_go_numerics(*args, **kw)
+    return _gcbc_apply(*args, **kw)
+
+
+def _addr(x):
+    if x is None:
+        return None
+    return x if isinstance(x, int) else x.data_ptr()
+
+
+def _gcbc_apply(drva_buffer, cm_buffer, drvb_buffer, qa, de, pressure, yaco, sbcc, umf, dudtmf, dcomp, dtwi, nbc,
+                mcd=None, stream=None):
+    d = dcomp if isinstance(dcomp, Dcomp) else Dcomp.of(*dcomp)
+    arr = lambda xs: (ctypes.c_void_p * 3)(*[_addr(x) for x in xs])
+    mc = nbc_array(mcd if mcd is not None else [[0] * 3, [0] * 3])
+    check(lib().cs_gcbc_apply(arr(drva_buffer), arr(cm_buffer), arr(drvb_buffer), ptr(qa), ptr(de), ptr(pressure),
+                              ptr(yaco), ptr(sbcc), (ctypes.c_double * 3)(*umf), (ctypes.c_double * 3)(*dudtmf), d,
+                              float(dtwi), nbc_array(nbc), mc, stream_ptr(stream)))
+
+
+def _gcbc_go_numerics(numerics_instance, cm, qa, de, pressure, yaco, sbcc, umf, dcomp, nbc, mcd=None,
+                      stream=None):
     d = dcomp if isinstance(dcomp, Dcomp) else Dcomp.of(*dcomp)
     cms = (ctypes.c_void_p * 3)(*[None if c is None else c.data_ptr() for c in cm])
     check(lib().cs_gcbc_go(numerics_instance.handle, cms, ptr(qa), ptr(de), ptr(pressure), ptr(yaco),

@@ -213,6 +213,26 @@ int cs_wall_condition_update(double *q, const int *npex, const double umf[3], cs
  * qout = qn - dtk * yaco * de (dtk = dt / (4 - k) for stage k). */
 int cs_rk_update(const double *qn, const double *de, const double *yaco, double dtk, double *qout,
                  size_t n, void *stream);
+/* gcbc_go (src/gcbc.hpp:86-186) with the reference's parameters, every face
+ * code of a single-rank block: non-reflective, inviscid / viscous wall and
+ * curvilinear-interface (GCIC) faces.  drva[a] ([2][5][F], the last
+ * derivatives' line-end values of axis a, e.g. a numerics object's drva
+ * buffers) is turned into characteristic form in place (gcbc_setup_kernel,
+ * src/cuda/kernels/gcbc.hpp:251-342: from drva on non-reflective faces, from
+ * the full J de elsewhere); for curvilinear-interface faces drvb[a] face ip
+ * receives drva[a] face 1-ip (the block is its own neighbour; the MPI
+ * exchange of src/gcbc.hpp:132-157, mcd unused); then de += sbcc * xtr2q *
+ * (cha - drva) on the first 4 planes of every such face (update kernels,
+ * :344-695).  cm[a]: [2][3][F] unit face normals; umf / dudtmf: frame
+ * velocity / acceleration; dtwi: 1/dt, the wall's relaxation rate.  Faces
+ * coded periodic or interface are skipped.  Reference defects fixed: the
+ * xtq2r typos, the accumulating output index, the plane of face 1 (dim-1),
+ * the thread part of the face index, and the wall update's missing
+ * subtraction of drva. */
+int cs_gcbc_apply(double *const drva[3], double *const cm[3], double *const drvb[3], const double *qa, double *de,
+                  const double *p, const double *yaco, const double *sbcc, const double umf[3],
+                  const double dudtmf[3], cs_dcomp d, double dtwi, const int nbc[2][3], const int mcd[2][3],
+                  void *stream);
 /* gcbc_go (src/gcbc.hpp:86-186) for non-reflective faces: characteristic
  * projection of the numerics object's drva, incoming acoustic waves removed,
  * de += sbcc * correction on the first 4 planes.  Faces coded periodic or

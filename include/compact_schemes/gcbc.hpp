@@ -1,5 +1,5 @@
-// compact_schemes/gcbc.hpp -- drop-in gcbc<Type, TypeIndex> and gcbc_go
-// (src/gcbc.hpp) over libcompact_b200, FP64, non-reflective faces.
+// compact_schemes/gcbc.hpp -- drop-in gcbc<Type, TypeIndex>, gcbc_go and
+// wall_condition_update (src/gcbc.hpp) over libcompact_b200, FP64.
 #pragma once
 
 #include "numerics_pc.hpp"
@@ -29,9 +29,27 @@ struct gcbc {
     Type *sbcc = nullptr;
 };
 
-// gcbc_go (src/gcbc.hpp:86-186).  drva comes from the numerics object that
-// computed the last flux derivatives; faces coded periodic / interface are
-// skipped; wall and curvilinear-interface faces are not in this build.
+// gcbc_go (src/gcbc.hpp:86-186) with the reference's parameter list: every
+// face code (non-reflective, inviscid / viscous wall, curvilinear interface)
+// of a single-rank block; drva_buffer is turned into characteristic form in
+// place as the reference does, drvb_buffer receives the GCIC exchange (the
+// block is its own neighbour; mcd is not needed).  FP64.
+template <typename Type>
+void gcbc_go(Type *drva_buffer[3], Type *cm_buffer[3], Type *drvb_buffer[3], Type *qa, Type *de, Type *pressure,
+             Type *yaco, Type *sbcc, t_point<Type> umf, t_point<Type> dudtmf, t_dcomp dcomp_info, Type dtwi,
+             int nbc[2][3], int mcd[2][3], cudaStream_t stream = nullptr) {
+    static_assert(std::is_same<Type, double>::value,
+                  "gcbc_go: FP64 (the drop-in physics path computes in double, see physics<Visc, Type>)");
+    const double u[3] = {umf.x, umf.y, umf.z};
+    const double a[3] = {dudtmf.x, dudtmf.y, dudtmf.z};
+    compact_b200::check(cs_gcbc_apply(drva_buffer, cm_buffer, drvb_buffer, qa, de, pressure, yaco, sbcc, u, a,
+                                      compact_b200::to_c(dcomp_info), dtwi, nbc, mcd, stream),
+                        "gcbc_go");
+}
+
+// gcbc_go for non-reflective faces with drva taken from the numerics object
+// that computed the last flux derivatives (the library's own shorthand; faces
+// coded periodic / interface are skipped).
 template <typename Type>
 void gcbc_go(numerics_pc<Type> *numerics_instance, Type *cm_buffer[3], Type *qa, Type *de,
              Type *pressure, Type *yaco, Type *sbcc, t_point<Type> umf, t_dcomp dcomp_info,

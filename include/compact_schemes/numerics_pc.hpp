@@ -72,7 +72,9 @@ struct numerics_pc {
     // numerics_pc::fill_buffers<min,max> (src/numerics_pc.hpp:231-287).
     template <unsigned int min_value, unsigned int max_value>
     void fill_buffers(Type *infield, int nrt, t_dcomp dcomp_info, cudaStream_t *streams) {
-        static_assert(std::is_same<Type, double>::value, "fill_buffers: double fields");
+        static_assert(std::is_same<Type, double>::value,
+                      "fill_buffers: FP64 fields (the interface exchange buffers are FP64; numerics_pc<float> "
+                      "derivatives use the single-rank periodic closure without them)");
         compact_b200::check(cs_fill_buffers(handle, infield, min_value, max_value, nrt,
                                             compact_b200::to_c(dcomp_info), streams ? streams[0] : nullptr),
                             "fill_buffers");

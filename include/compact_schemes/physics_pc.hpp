@@ -18,7 +18,14 @@ struct t_heat_fluxes {
 
 template <bool EnableViscous, typename Type>
 struct physics {
-    static_assert(std::is_same<Type, double>::value, "physics<Visc, Type>: FP64 build");
+    // The reference driver instantiates physics<true, float>; this drop-in path
+    // computes the fluxes, stresses, time step and RHS in FP64 only: the
+    // hot path's parity bar is FP64 (1e-12 against the host path), and the
+    // library's FP32 arithmetic lives in the fused mixed-precision step
+    // (CS_PREC_MIXED) and in numerics_pc<float>::deriv1d/deriv2d.
+    static_assert(std::is_same<Type, double>::value,
+                  "physics<Visc, Type>: the drop-in physics path is FP64 (use double; FP32 runs in the fused "
+                  "solver's CS_PREC_MIXED form and numerics_pc<float> derivatives)");
 
     explicit physics(t_dcomp dcomp_info) : d(dcomp_info) {
         compact_b200::check(cs_physics_create(&handle, compact_b200::to_c(d), EnableViscous ? 1 : 0),

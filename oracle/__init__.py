@@ -73,6 +73,8 @@ def lib():
         L.or_grid_metrics.argtypes = [vp, vp, i32, i32, i32, vp, vp, vp, vp, vp]
         L.or_grid_metrics.restype = i32
         L.or_tgv_init.argtypes = [vp, i32, i32, i32, f64, f64, ctypes.c_uint64]
+        L.or_gcbc_go.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, i32, f64, vp]
+        L.or_gcbc_go.restype = i32
         L.or_fourier_field.argtypes = [i32, i32, i32, ctypes.c_uint64, i32, vp, vp]
         L.or_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.or_noise.restype = f64
@@ -231,6 +233,20 @@ def gcbc_x(rhs_arr, drva_x, cm, q, sbcc, metrics, dims, nbc, umf=(0.0, 0.0, 0.0)
                          _p(u), lxi, let, lze, nbp)
     if rc:
         raise ValueError("or_gcbc_x failed")
+
+
+def gcbc_go(drva, cm, drvb, qa, de, p, yaco, sbcc, umf, dudtmf, dims, dtwi, nbc):
+    """In place: drva[a] -> characteristic form, drvb[a] filled, de updated
+    (or_gcbc_go).  drva, cm, drvb: lists of 3 float64 arrays (or None)."""
+    lxi, let, lze = dims
+    arr = lambda xs: (ctypes.c_void_p * 3)(*[None if x is None else x.ctypes.data for x in xs])
+    nb, nbp = _ip(nbc)
+    u = np.asarray(umf, dtype=np.float64)
+    du = np.asarray(dudtmf, dtype=np.float64)
+    rc = lib().or_gcbc_go(arr(drva), arr(cm), arr(drvb), _p(qa), _p(de), _p(p), _p(yaco), _p(sbcc), _p(u),
+                          _p(du), lxi, let, lze, float(dtwi), nbp)
+    if rc:
+        raise ValueError("or_gcbc_go failed (%d)" % rc)
 
 
 def rk_step(q, mu, metrics, dims, nbc, viscous=True, dt=0.0, cfl=0.5, gcbc=False,

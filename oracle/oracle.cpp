@@ -703,6 +703,164 @@ int or_gcbc_x(double *rhs, const double *drva_x, const double *cm, const double 
     return 0;
 }
 
+// Characteristic state of one face point (gcbc_vgpr::eleme,
+// src/cuda/kernels/gcbc.hpp:43-57): face normal c, density, momenta, pressure.
+struct GcPt {
+    double c[3], ve[3], hv2, ao, aoi, vn, vs;
+};
+static GcPt gc_eleme(const double c[3], double rho, const double m[3], double pp, const double umf[3]) {
+    GcPt g;
+    const double rhoi = 1.0 / rho;
+    for (int k = 0; k < 3; ++k) g.c[k] = c[k];
+    g.ao = std::sqrt(kGam * rhoi * pp);
+    g.aoi = 1.0 / g.ao;
+    g.ve[0] = rhoi * m[0];
+    g.ve[1] = rhoi * m[1];
+    g.ve[2] = rhoi * m[2];
+    g.hv2 = 0.5 * (g.ve[0] * g.ve[0] + g.ve[1] * g.ve[1] + g.ve[2] * g.ve[2]);
+    g.vn = c[0] * g.ve[0] + c[1] * g.ve[1] + c[2] * g.ve[2];
+    g.vs = c[0] * umf[0] + c[1] * umf[1] + c[2] * umf[2];
+    return g;
+}
+// xtq2r (conservative -> characteristic, :109-150) with its three typos fixed.
+static void gc_xtq2r(const GcPt &g, double L[5][5]) {
+    const double *c = g.c, *ve = g.ve;
+    const double ho = kGamm1 * g.aoi * g.aoi, bo = 1.0 - ho * g.hv2, co = g.aoi * g.vn;
+    const double dm[3] = {g.aoi * c[0], g.aoi * c[1], g.aoi * c[2]};
+    const double rv[3] = {ho * ve[0], ho * ve[1], ho * ve[2]};
+    const double t[5][5] = {
+        {bo * c[0] + dm[1] * ve[2] - dm[2] * ve[1], c[0] * rv[0], c[0] * rv[1] + dm[2], c[0] * rv[2] - dm[1], -ho * c[0]},
+        {bo * c[1] + dm[2] * ve[0] - dm[0] * ve[2], c[1] * rv[0] - dm[2], c[1] * rv[1], c[1] * rv[2] + dm[0], -ho * c[1]},
+        {bo * c[2] + dm[0] * ve[1] - dm[1] * ve[0], c[2] * rv[0] + dm[1], c[2] * rv[1] - dm[0], c[2] * rv[2], -ho * c[2]},
+        {1.0 - bo - co, dm[0] - rv[0], dm[1] - rv[1], dm[2] - rv[2], ho},
+        {1.0 - bo + co, -dm[0] - rv[0], -dm[1] - rv[1], -dm[2] - rv[2], ho}};
+    std::memcpy(L, t, sizeof t);
+}
+// xtr2q (characteristic -> conservative, :59-107).
+static void gc_xtr2q(const GcPt &g, double S[5][5]) {
+    const double *c = g.c, *ve = g.ve;
+    const double bo = g.hv2 + kHamm1 * g.ao * g.ao, co = g.ao * g.vn;
+    const double dm[3] = {g.ao * c[0], g.ao * c[1], g.ao * c[2]};
+    const double t[5][5] = {
+        {c[0], c[1], c[2], 0.5, 0.5},
+        {c[0] * ve[0], c[1] * ve[0] - dm[2], c[2] * ve[0] + dm[1], 0.5 * (ve[0] + dm[0]), 0.5 * (ve[0] + dm[0]) - dm[0]},
+        {c[0] * ve[1] + dm[2], c[1] * ve[1], c[2] * ve[1] - dm[0], 0.5 * (ve[1] + dm[1]), 0.5 * (ve[1] + dm[1]) - dm[1]},
+        {c[0] * ve[2] - dm[1], c[1] * ve[2] + dm[0], c[2] * ve[2], 0.5 * (ve[2] + dm[2]), 0.5 * (ve[2] + dm[2]) - dm[2]},
+        {g.hv2 * c[0] + dm[2] * ve[1] - dm[1] * ve[2], g.hv2 * c[1] + dm[0] * ve[2] - dm[2] * ve[0],
+         g.hv2 * c[2] + dm[1] * ve[0] - dm[0] * ve[1], 0.5 * (bo + co), 0.5 * (bo + co) - co}};
+    std::memcpy(S, t, sizeof t);
+}
+static void gc_matvec(const double A[5][5], const double *x, double *y) {
+    for (int r = 0; r < 5; ++r) {
+        double v = 0.0;
+        for (int k = 0; k < 5; ++k) v += A[r][k] * x[k];
+        y[r] = v;
+    }
+}
+
+// Point `fi` of face ip of axis a: linear index of its face point and the
+// stride into the block (face index convention of the derivative's drva).
+static int64_t gc_face_point(int a, int ip, int64_t fi, int lxi, int let, int lze, int64_t &stride) {
+    int64_t base;
+    int dim;
+    if (a == 0) { base = fi * lxi; stride = 1; dim = lxi; }
+    else if (a == 1) { base = (fi / lxi) * (int64_t)lxi * let + fi % lxi; stride = lxi; dim = let; }
+    else { base = fi; stride = (int64_t)lxi * let; dim = lze; }
+    return base + (int64_t)(ip ? dim - 1 : 0) * stride;
+}
+
+// gcbc_go (src/gcbc.hpp:86-186) on every face, single rank: gcbc_setup_kernel
+// (src/cuda/kernels/gcbc.hpp:251-342) turns drva of non-reflective, wall and
+// curvilinear-interface faces into characteristic form in place (from drva,
+// flag 1, on non-reflective faces; from the full right-hand side J de, flag 0,
+// on the others); the GCIC exchange copies drva of face 1-ip into drvb of
+// face ip for curvilinear-interface faces (the block is its own neighbour,
+// as mpi exchange::trigger pairs them, src/gcbc.hpp:132-157); then the
+// update kernels (:344-695) add sbcc * xtr2q * (cha - drva) to de on mbci
+// planes.  Defects fixed as in or_gcbc_x, and the wall update subtracts drva
+// from cha as the other two do (gcbc_update_wall_kernel adds xtr2q * cha,
+// the whole characteristic right-hand side, :531-545).
+int or_gcbc_go(double *drva[3], const double *cm[3], double *drvb[3], const double *qa, double *de,
+               const double *p, const double *yaco, const double *sbcc, const double umf[3],
+               const double dudtmf[3], int lxi, int let, int lze, double dtwi, const int nbc[2][3]) {
+    const int64_t n = (int64_t)lxi * let * lze;
+    const int dims[3] = {lxi, let, lze};
+    auto active = [](int np) {
+        return np == kBcNonReflective || np == 20 || np == 25 || np == 30;
+    };
+    for (int a = 0; a < 3; ++a) {
+        const int64_t F = a == 0 ? (int64_t)let * lze : (a == 1 ? (int64_t)lxi * lze : (int64_t)lxi * let);
+        for (int ip = 0; ip < 2; ++ip) {
+            const int np = nbc[ip][a];
+            if (!active(np)) continue;
+            if (dims[a] < 2 || !drva[a] || !cm[a]) return -1;
+            const bool flag = np == kBcNonReflective;
+            for (int64_t fi = 0; fi < F; ++fi) {
+                int64_t stride;
+                const int64_t idx = gc_face_point(a, ip, fi, lxi, let, lze, stride);
+                const double c[3] = {cm[a][(ip * 3 + 0) * F + fi], cm[a][(ip * 3 + 1) * F + fi],
+                                     cm[a][(ip * 3 + 2) * F + fi]};
+                const double m[3] = {qa[n + idx], qa[2 * n + idx], qa[3 * n + idx]};
+                const GcPt g = gc_eleme(c, qa[idx], m, p[idx], umf);
+                double L[5][5], src[5], cha[5];
+                gc_xtq2r(g, L);
+                for (int v = 0; v < 5; ++v)
+                    src[v] = yaco[idx] * (flag ? drva[a][(ip * 5 + v) * F + fi] : de[v * n + idx]);
+                gc_matvec(L, src, cha);
+                for (int v = 0; v < 5; ++v) drva[a][(ip * 5 + v) * F + fi] = cha[v];
+            }
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        const int64_t F = a == 0 ? (int64_t)let * lze : (a == 1 ? (int64_t)lxi * lze : (int64_t)lxi * let);
+        for (int ip = 0; ip < 2; ++ip)
+            if (nbc[ip][a] == 30) {
+                if (!drvb[a]) return -1;
+                std::memcpy(drvb[a] + (int64_t)ip * 5 * F, drva[a] + (int64_t)(1 - ip) * 5 * F, 5 * F * sizeof(double));
+            }
+    }
+    for (int a = 0; a < 3; ++a) {
+        const int64_t F = a == 0 ? (int64_t)let * lze : (a == 1 ? (int64_t)lxi * lze : (int64_t)lxi * let);
+        for (int ip = 0; ip < 2; ++ip) {
+            const int np = nbc[ip][a];
+            if (!active(np)) continue;
+            const double ra0 = 1.0 - 2.0 * ip;
+            for (int64_t fi = 0; fi < F; ++fi) {
+                int64_t stride;
+                const int64_t idx = gc_face_point(a, ip, fi, lxi, let, lze, stride);
+                const double c[3] = {cm[a][(ip * 3 + 0) * F + fi], cm[a][(ip * 3 + 1) * F + fi],
+                                     cm[a][(ip * 3 + 2) * F + fi]};
+                const double m[3] = {qa[n + idx], qa[2 * n + idx], qa[3 * n + idx]};
+                const GcPt g = gc_eleme(c, qa[idx], m, p[idx], umf);
+                double dr[5], cha[5], dq[5], S[5][5];
+                for (int v = 0; v < 5; ++v) cha[v] = dr[v] = drva[a][(ip * 5 + v) * F + fi];
+                if (np == kBcNonReflective) {
+                    if (ra0 * (g.vn + g.vs + g.ao) > 0) cha[3] = 0.0;
+                    if (ra0 * (g.vn + g.vs - g.ao) > 0) cha[4] = 0.0;
+                } else if (np == 30) {
+                    double dh[5];
+                    for (int v = 0; v < 5; ++v) dh[v] = drvb[a][(ip * 5 + v) * F + fi];
+                    if (ra0 * (g.vn + g.vs) > 0) { cha[0] = dh[0]; cha[1] = dh[1]; cha[2] = dh[2]; }
+                    if (ra0 * (g.vn + g.vs + g.ao) > 0) cha[3] = dh[3];
+                    if (ra0 * (g.vn + g.vs - g.ao) > 0) cha[4] = dh[4];
+                } else {
+                    const double acc = c[0] * dudtmf[0] + c[1] * dudtmf[1] + c[2] * dudtmf[2];
+                    cha[3 + ip] = cha[4 - ip] + 2.0 * ra0 * g.aoi * qa[idx] * (acc + dtwi * (g.vn + g.vs));
+                }
+                for (int v = 0; v < 5; ++v) cha[v] -= dr[v];
+                gc_xtr2q(g, S);
+                gc_matvec(S, cha, dq);
+                const int iq = 1 - 2 * ip;
+                for (int ii = 0; ii < kMbci && ii < dims[a]; ++ii) {
+                    const int64_t o = idx + (int64_t)ii * iq * stride;
+                    for (int v = 0; v < 5; ++v) de[v * n + o] += sbcc[o] * dq[v];
+                }
+            }
+        }
+    }
+    return 0;
+}
+
 // One step of the driver's RK loop (driver/canard.cu:132-224), with the
 // update the reference leaves empty (movef, src/physics_base.hpp:147-150):
 // four stages q^(k) = q^n - dt/(nkrk-k) * J * rhs(q^(k-1)), k = 0..3

@@ -137,6 +137,17 @@ double or_rk_stage(const double *qn, const double *qin, double *qout, int k, dou
 int or_grid_metrics(const double *xyz, const double period[3][3], int lxi, int let, int lze,
                     const int ndf[2][3], double *xim, double *etm, double *zem, double *yaco);
 
+/* gcbc_go (src/gcbc.hpp:86-186) on all faces of a single-rank block:
+ * non-reflective (10), inviscid / viscous wall (20 / 25) and curvilinear
+ * interface (30) faces; drva[a] ([2][5][F], in: line-end derivatives, out:
+ * characteristic form), cm[a] ([2][3][F] unit normals), drvb[a] ([2][5][F],
+ * out: the neighbour's characteristic values, here face 1-ip of the block
+ * itself); de [5][n] updated on kMbci planes per face with weights sbcc [n].
+ * Returns 0, -1 on a missing buffer. */
+int or_gcbc_go(double *drva[3], const double *cm[3], double *drvb[3], const double *qa, double *de,
+               const double *p, const double *yaco, const double *sbcc, const double umf[3],
+               const double dudtmf[3], int lxi, int let, int lze, double dtwi, const int nbc[2][3]);
+
 /* Taylor-Green initial state on a periodic [0,2pi)^3 grid (CANARD units:
  * rho0 = 1, c_inf = 1, p0 = 1/gamma), density noise amp*U(-1,1) from the
  * counter-based generator or_noise. */

@@ -227,3 +227,93 @@ def test_fluxes_pre_against_reference_fp64_kernel(cuda):
     for c in range(15):
         assert rel(ours[c], th[c]) < 1e-12, c
     assert rel(ours_de4, r_de.cpu().numpy()[4 * n:]) < 1e-12
+
+
+def test_reference_driver_sequence_runs(cuda, tmp_path):
+    """The reference driver's loop through the drop-in headers (non-reflective
+    x faces, viscous y walls, periodic z; gcbc_go with the reference's
+    parameter list), three RK steps on the B200."""
+    from test_dropin_build import build_demo
+    exe = build_demo(str(tmp_path / "driver_sequence"), "driver_sequence.cpp")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
+
+
+def _gcbc_case(dims, seed):
+    """A smooth compressible state, its pressure, a right-hand side, line-end
+    derivatives, unit face normals (tilted), Jacobian and boundary weights."""
+    r = np.random.default_rng(seed)
+    n = int(np.prod(dims))
+    q = O.tgv_init(dims, 0.3, 1e-3, seed)
+    q[3 * n:4 * n] = 0.05 * q[:n] * np.sin(np.arange(n) * 0.01)  # nonzero w
+    de_t, p = O.thermo(q)
+    de = 0.1 * r.standard_normal(5 * n)
+    yaco = 1.0 + 0.2 * r.random(n)
+    sbcc = r.random(n)
+    F = (dims[1] * dims[2], dims[0] * dims[2], dims[0] * dims[1])
+    drva, cm = [], []
+    for a in range(3):
+        drva.append(r.standard_normal(10 * F[a]))
+        c = np.zeros((2, 3, F[a]))
+        c[:, a, :] = 1.0
+        c += 0.2 * r.standard_normal((2, 3, F[a]))
+        c /= np.linalg.norm(c, axis=1, keepdims=True)
+        cm.append(c.ravel().copy())
+    return q, p, de, yaco, sbcc, drva, cm, F
+
+
+@pytest.mark.parametrize("nbc", [[[10, 20, 30], [25, 10, 30]], [[30, 25, 10], [30, 20, 10]],
+                                 [[20, 45, 25], [10, 45, 20]]])
+def test_gcbc_apply_all_face_codes_match_oracle(cuda, nbc):
+    """cs_gcbc_apply (gcbc_go with the reference's parameters) on every face
+    code: non-reflective (10), inviscid / viscous wall (20 / 25), curvilinear
+    interface (30) with the single-rank GCIC exchange, on all three axes,
+    tilted face normals, frame velocity and acceleration: de, the
+    characteristic drva and drvb against the oracle at 1e-12."""
+    import torch
+    import compact_schemes_b200 as cs
+    dims = (20, 16, 12)
+    q, p, de, yaco, sbcc, drva, cm, F = _gcbc_case(dims, 4)
+    umf, dudtmf, dtwi = (0.02, -0.01, 0.015), (0.3, -0.2, 0.1), 25.0
+    drvb = [np.zeros(10 * f) for f in F]
+    de_o, drva_o, drvb_o = de.copy(), [x.copy() for x in drva], [x.copy() for x in drvb]
+    O.gcbc_go(drva_o, cm, drvb_o, q, de_o, p, yaco, sbcc, umf, dudtmf, dims, dtwi, nbc)
+    d_drva = [dev(x) for x in drva]
+    d_drvb = [dev(x) for x in drvb]
+    d_cm = [dev(x) for x in cm]
+    d_de = dev(de)
+    cs.gcbc_go(d_drva, d_cm, d_drvb, dev(q), d_de, dev(p), dev(yaco), dev(sbcc), umf, dudtmf, dims, dtwi, nbc,
+               [[0] * 3, [0] * 3])
+    torch.cuda.synchronize()
+    corr_o = de_o - de
+    corr_g = d_de.cpu().numpy() - de
+    assert np.abs(corr_o).max() > 0
+    assert np.abs(corr_g - corr_o).max() / np.abs(corr_o).max() < 1e-12
+    for a in range(3):
+        assert rel(d_drva[a].cpu().numpy(), drva_o[a]) < 1e-12, a
+        if np.abs(drvb_o[a]).max() > 0:
+            assert rel(d_drvb[a].cpu().numpy(), drvb_o[a]) < 1e-12, a
+
+
+def test_gcbc_apply_non_reflective_equals_numerics_path(cuda):
+    """On non-reflective faces the reference-signature path equals the
+    numerics-object path (fused setup + update) to rounding."""
+    import torch
+    import compact_schemes_b200 as cs
+    dims = (20, 16, 12)
+    q, p, de, yaco, sbcc, drva, cm, F = _gcbc_case(dims, 5)
+    nbc = [[10, 10, 10], [10, 10, 10]]
+    nm = cs.numerics_pc(dims, nbc)
+    nm.deriv_setup()
+    for a in range(3):
+        dp, _, _ = nm.buffers(a)
+        device_view(dp, 10 * F[a]).copy_(dev(drva[a]))
+    d1 = dev(de)
+    cs.gcbc_go(nm, [dev(c) for c in cm], dev(q), d1, dev(p), dev(yaco), dev(sbcc), (0.01, 0.0, 0.0), dims, nbc)
+    d2 = dev(de)
+    cs.gcbc_go([dev(x) for x in drva], [dev(c) for c in cm], [None] * 3, dev(q), d2, dev(p), dev(yaco),
+               dev(sbcc), (0.01, 0.0, 0.0), (0.0, 0.0, 0.0), dims, 10.0, nbc)
+    torch.cuda.synchronize()
+    c1, c2 = (d1 - dev(de)).cpu().numpy(), (d2 - dev(de)).cpu().numpy()
+    assert np.abs(c1).max() > 0
+    assert np.abs(c1 - c2).max() / np.abs(c1).max() < 1e-13
