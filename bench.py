@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--no-reference-kernels", action="store_true")
     p.add_argument("--no-config1", action="store_true")
     p.add_argument("--no-dropin", action="store_true")
+    p.add_argument("--no-filter", action="store_true")
     return p.parse_args()
 
 
@@ -535,6 +536,47 @@ def dropin_section(args, fused_ms_per_step, stages=8):
             "stages": stages}
 
 
+def filter_section(args, plain_ms_per_step, steps=20):
+    """The compact filter inside the time step (CS_FILTER_STEP: after every RK
+    step, alpha_f 0.45, all five conserved fields along x, y and z) on the
+    headline 256^3 workload: step time against the plain step, and each
+    filter pass against 80 B/pt (five fields read and written)."""
+    import torch
+    import compact_schemes_b200 as cs
+    from compact_schemes_b200.solver import FILTER_STEP
+    n = args.n
+    lmx = n ** 3
+    s = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, filter=FILTER_STEP, alpha_f=0.45))
+    q = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
+    cs.tgv_init(q, (n, n, n), MACH, 1e-4, 0)
+    s.autotune(q, reps=1)
+    for _ in range(args.warmup):
+        s.step(q)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        s.step(q)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    s.profile_begin()
+    for _ in range(2):
+        s.step(q)
+    prof = s.profile_end()
+    s.close()
+    del q
+    torch.cuda.empty_cache()
+    hbm, _ = peaks()
+    fms, fl = prof["filter"]
+    per = fms / fl
+    return {"workload": "taylor_green_%d^3 FP64, filter after every RK step (alpha_f 0.45)" % n,
+            "ms_per_step": ms, "plain_ms_per_step": plain_ms_per_step, "filter_share": 1 - plain_ms_per_step / ms,
+            "value": lmx * 4 / (ms * 1e-3) / 1e6, "unit": UNIT,
+            "filter_pass_ms_per_launch": per, "filter_pass_bytes_per_point": 80,
+            "filter_pass_frac": 80 * lmx / (per * 1e-3) / 1e9 / hbm}
+
+
 def config1_section(args, reps=20):
     """The derivative-and-filter workload: the 64^3 non-periodic [0,1]^3
     field of 8 Fourier modes (MT19937-64 seed 0), physical closures on all
@@ -885,7 +927,7 @@ def run_ours(args):
                "sample": "1 RK stage of the %d^3 Taylor-Green box in %.1f s (FP64 oracle, "
                          "C++/OpenMP restatement of the reference kernels)" % (n, t)}
 
-    ensemble = adjoint = mixed512 = curvilinear = refk = cfg1 = dropin = None
+    ensemble = adjoint = mixed512 = curvilinear = refk = cfg1 = dropin = filt = None
     if rank == 0 and world == 1:
         s.close()
         if not args.no_reference_kernels:
@@ -896,6 +938,8 @@ def run_ours(args):
         if not args.no_dropin:
             dropin = dropin_section(args, t_ms / args.steps)
             torch.cuda.empty_cache()
+        if not args.no_filter:
+            filt = filter_section(args, t_ms / args.steps)
         if not args.no_curvilinear:
             curvilinear = curvilinear_section(args, t_ms / args.steps)
             torch.cuda.empty_cache()
@@ -920,6 +964,7 @@ def run_ours(args):
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed,
                 "mixed_512_gcbc": mixed512, "ensemble": ensemble, "adjoint": adjoint,
                 "curvilinear": curvilinear, "reference_kernels": refk, "config1": cfg1, "dropin": dropin,
+                "filter": filt,
                 "gpu_launches": 24 * args.steps, "clocks": clocks,
                 "passes": per_pass,
                 "stage_model": {"bytes_per_point": STAGE_BYTES, "ms_per_stage": stage_ms,

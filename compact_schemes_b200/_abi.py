@@ -67,6 +67,8 @@ def declare(L):
     L.cs_ensemble_step.argtypes = [vp, vp, vp]
     L.cs_ensemble_last_dt.argtypes = [vp, ctypes.POINTER(f64)]
     L.cs_ensemble_set_tuning.argtypes = [vp, pt]
+    L.cs_ensemble_set_wait.argtypes = [vp, ctypes.c_longlong, i32]
+    L.cs_ensemble_set_wait.restype = i32
     L.cs_ensemble_get_tuning.argtypes = [vp, pt]
     L.cs_ensemble_autotune.argtypes = [vp, vp, i32, pt, ctypes.POINTER(f64), vp]
     for name in ("cs_ensemble_create", "cs_ensemble_destroy", "cs_ensemble_state_size", "cs_ensemble_box_offset",

@@ -36,6 +36,9 @@ struct cs_ensemble {
     cudaGraphExec_t graph = nullptr;
     const double *graph_q = nullptr;
     cudaStream_t graph_stream = nullptr;
+    // dependency wait: poll limit and extra required items (cs_ensemble_set_wait)
+    long long poll_limit = csb::kEnsWaitPolls;
+    int wait_bias = 0;
 };
 
 namespace csb {
@@ -124,6 +127,8 @@ static int ens_run_step(cs_ensemble *e, double *q, cudaStream_t st) {
     EnsArgs a{};
     a.boxes = e->dbox;
     a.err = e->ctl;
+    a.poll_limit = e->poll_limit;
+    a.wait_bias = e->wait_bias;
     a.queue = e->ctl + 1;
     a.done = e->ctl + 2;
     a.q = q;
@@ -318,6 +323,15 @@ int cs_ensemble_last_dt(cs_ensemble *e, double *dt_host) {
         CSB_CUDA(cudaMemset(e->ctl, 0, sizeof(int)));
         return set_error(CS_ERR_TIMEOUT, "ensemble: the dependency wait of work item %d ran out", err - 1);
     }
+    return CS_OK;
+}
+
+int cs_ensemble_set_wait(cs_ensemble *e, long long poll_limit, int extra) {
+    if (!e) return set_error(CS_ERR_INVALID, "null argument");
+    if (poll_limit < 1 || extra < 0) return set_error(CS_ERR_INVALID, "poll_limit %lld, extra %d", poll_limit, extra);
+    e->poll_limit = poll_limit;
+    e->wait_bias = extra;
+    if (e->graph) { cudaGraphExecDestroy(e->graph); e->graph = nullptr; }
     return CS_OK;
 }
 

@@ -62,6 +62,8 @@ struct EnsArgs {
     int *queue;      // next item number
     int *done;       // [nbox][kEnsPhases] finished items
     int *err;        // 0, or 1 + the item whose dependency wait ran out
+    long long poll_limit;  // polls of a dependency wait before it gives up
+    int wait_bias;   // finished items a wait needs beyond its count (0; > 0 only to test the timeout)
     double *q;       // packed state q^n (updated in place by the last stage)
     double *q1;      // packed intermediate stage state
     double *grad;    // packed gradients [12][lmx] per box
@@ -177,8 +179,8 @@ __global__ void __launch_bounds__(TL * 32, TL == 8 ? 2 : 4) k_ensemble_stage(con
             if (sg.wait_count > 0) {
                 const int *dp = a.done + sg.box * kEnsPhases + sg.phase - 1;
                 long long polls = 0;
-                while (ens_load_acquire(dp) < sg.wait_count) {
-                    if (++polls > kEnsWaitPolls) { ok = 0; break; }
+                while (ens_load_acquire(dp) < sg.wait_count + a.wait_bias) {
+                    if (++polls > a.poll_limit) { ok = 0; break; }
                     __nanosleep(100);
                 }
                 if (!ok) atomicCAS(a.err, 0, 1 + it);

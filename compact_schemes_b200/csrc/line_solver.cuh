@@ -152,37 +152,12 @@ __device__ __forceinline__ CT get_at(const CT (&d)[LT], int t) {
     return r;
 }
 
-// One of the eight interface-closure sums of a line held in LineLayout<LT>
-// order in shared memory (single-rank periodic closure, ndf = 1 on both
-// faces), summed in index order k = 0..7 exactly as a serial evaluation:
-//   d = 0 / 1: sum_k pbci[k] f[k] / pbci[8+k] f[k]           (row 0 / 1, own end)
-//   d = 2 / 3: sum_k pbco[k] f[n-1-k] / pbco[8+k] f[n-1-k]   (row 0 / 1, far end)
-//   d = 4 / 5: sum_k pbci[k] f[n-1-k] / pbci[8+k] f[n-1-k]   (row n-1 / n-2, own end)
-//   d = 6 / 7: sum_k pbco[k] f[k] / pbco[8+k] f[k]           (row n-1 / n-2, far end)
-template <int LT, typename CT, typename FT>
-__device__ __forceinline__ CT interface_sum(const FT *f, int n, int d, const Coeffs &cf) {
-    using L = LineLayout<LT>;
-    const bool bci = d < 2 || d == 4 || d == 5;
-    const bool asc = d < 2 || d >= 6;
-    const bool second = (d & 1) != 0;
-    CT s = CT(0);
-#pragma unroll
-    for (int k = 0; k < kLmd; ++k) {
-        const double c = bci ? (second ? cf.pbci[kLmd + k] : cf.pbci[k]) : (second ? cf.pbco[kLmd + k] : cf.pbco[k]);
-        s += xmul(CT(c), CT(f[L::pos(asc ? k : n - 1 - k)]));
-    }
-    return s;
-}
-
 // Right-hand side of the compact derivative for the rows of this lane,
 // restating build_system (src/cuda/kernels/numerics_device_pc.hpp:176-293):
 // interior aa*(f[j+1]-f[j-1]) + bb*(f[j+2]-f[j-2]); physical closure rows
 // (ndf = 0) or interface closure rows (ndf = 1: 8-point pbci sums plus the
 // received pbco sums; `recv4` = {row0, row1, row n-1, row n-2} received
-// values, or, when it is null, the line's own far-end sums for single-rank
-// periodic).  Without received values the eight interface sums are formed by
-// lanes 0-7 in parallel (interface_sum) and broadcast by shuffles, each in the
-// same operation order as a serial evaluation.  All 32 lanes must call it.
+// values, or the line's own far-end sums for single-rank periodic).
 // `f` is the line in LineLayout<LT> order in shared memory.
 template <int LT, typename CT, typename FT>
 __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nstart, int nend,
@@ -201,20 +176,6 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
     for (int t = 0; t < LT; ++t)
         d[t] = (j0 + t < n) ? xmul(CT(kAa), w[t + 3] - w[t + 1]) + xmul(CT(kBb), w[t + 4] - w[t]) : CT(0);
 
-    // single-rank interface sums, lane-parallel (warp-uniform condition):
-    // lanes 0, 1, 4, 5 add the own-end and far-end sums of rows 0, 1, n-1,
-    // n-2; lane 0 takes rows 0 and 1, every other lane rows n-1 and n-2 (the
-    // owners of rows n-1, n-2 are never lane 0 for lines of 8 or more points)
-    CT sa = CT(0), sb = CT(0);
-    const bool own_sums = !recv4_or_null && (nstart != 0 || nend != 0);
-    if (own_sums) {
-        const CT dv = lane < 8 ? interface_sum<LT, CT, FT>(f, n, lane, cf) : CT(0);
-        const CT x = dv + __shfl_down_sync(0xffffffffu, dv, 2);
-        const int src = lane == 0 ? 0 : 4;
-        sa = __shfl_sync(0xffffffffu, x, src);
-        sb = __shfl_sync(0xffffffffu, x, src + 1);
-    }
-
     const bool own_lo = lane == 0;
     const int own_hi1 = (n - 1) / LT, own_hi2 = (n - 2) / LT;
     if (own_lo || lane == own_hi1 || lane == own_hi2) {
@@ -224,11 +185,19 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
             if (nstart == 0) {
                 d[0] = xmul(CT(kAb00), f0) + xmul(CT(kAb01), f1) + xmul(CT(kAb02), f2);
                 d[1] = xmul(CT(kAb10), f2 - f0);
-            } else if (own_sums) {
-                d[0] = sa;
-                d[1] = sb;
             } else {
-                const CT r0 = recv4_or_null[0], r1 = recv4_or_null[1];
+                CT r0, r1;
+                if (recv4_or_null) {
+                    r0 = recv4_or_null[0];
+                    r1 = recv4_or_null[1];
+                } else {
+                    r0 = CT(0);
+                    r1 = CT(0);
+#pragma unroll
+                    for (int k = 0; k < kLmd; ++k) r0 += xmul(CT(cf.pbco[k]), CT(f[L::pos(n - 1 - k)]));
+#pragma unroll
+                    for (int k = 0; k < kLmd; ++k) r1 += xmul(CT(cf.pbco[kLmd + k]), CT(f[L::pos(n - 1 - k)]));
+                }
                 CT s0 = CT(0), s1 = CT(0);
 #pragma unroll
                 for (int k = 0; k < kLmd; ++k) s0 += xmul(CT(cf.pbci[k]), CT(f[L::pos(k)]));
@@ -244,11 +213,19 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
             if (nend == 0) {
                 e1 = -(xmul(CT(kAb00), g0) + xmul(CT(kAb01), g1) + xmul(CT(kAb02), g2));
                 e2 = xmul(-CT(kAb10), g2 - g0);
-            } else if (own_sums) {
-                e1 = -sa;
-                e2 = -sb;
             } else {
-                const CT r2 = recv4_or_null[2], r3 = recv4_or_null[3];
+                CT r2, r3;
+                if (recv4_or_null) {
+                    r2 = recv4_or_null[2];
+                    r3 = recv4_or_null[3];
+                } else {
+                    r2 = CT(0);
+                    r3 = CT(0);
+#pragma unroll
+                    for (int k = 0; k < kLmd; ++k) r2 += xmul(CT(cf.pbco[k]), CT(f[L::pos(k)]));
+#pragma unroll
+                    for (int k = 0; k < kLmd; ++k) r3 += xmul(CT(cf.pbco[kLmd + k]), CT(f[L::pos(k)]));
+                }
                 CT s0 = CT(0), s1 = CT(0);
 #pragma unroll
                 for (int k = 0; k < kLmd; ++k) s0 += xmul(CT(cf.pbci[k]), CT(f[L::pos(n - 1 - k)]));

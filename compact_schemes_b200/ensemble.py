@@ -72,6 +72,11 @@ class Ensemble:
         check(lib().cs_ensemble_last_dt(self._h, out))
         return list(out)
 
+    def set_wait(self, poll_limit=20000000, extra=0):
+        """Dependency-wait limit and, for tests of the timeout path, `extra`
+        finished items every wait needs beyond what the queue produces."""
+        check(lib().cs_ensemble_set_wait(self._h, int(poll_limit), int(extra)))
+
     def tuning(self):
         t = EnsembleTuning()
         check(lib().cs_ensemble_get_tuning(self._h, ctypes.byref(t)))

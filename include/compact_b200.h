@@ -392,6 +392,15 @@ int cs_ensemble_step(cs_ensemble *e, double *q, void *stream);
  * dependency wait of the work queue ran out since the previous check. */
 int cs_ensemble_last_dt(cs_ensemble *e, double *dt_host);
 int cs_ensemble_set_tuning(cs_ensemble *e, const cs_ensemble_tuning *t);
+/* Failure-detection hook of the stage kernel's dependency wait: a wait gives
+ * up after poll_limit polls of about 100 ns (default 2e7), records the work
+ * item in the error word, skips the item and lets the launch finish, and
+ * cs_ensemble_last_dt returns CS_ERR_TIMEOUT (the step's state is then
+ * invalid).  extra > 0 makes every wait need `extra` more finished items than
+ * the queue can produce, so every dependent item times out: a test of that
+ * path that faults nothing.  (default_polls, 0) restores the default. */
+#define CS_ENSEMBLE_DEFAULT_POLLS 20000000LL
+int cs_ensemble_set_wait(cs_ensemble *e, long long poll_limit, int extra);
 int cs_ensemble_get_tuning(const cs_ensemble *e, cs_ensemble_tuning *t);
 /* Autotuner: times `reps` steps of every candidate tuning (tile width x tiles
  * per work item x queue lag) on a scratch copy of q (q is not modified),

@@ -126,3 +126,30 @@ def test_ensemble_rejects_unsupported(cuda):
         cs.Ensemble(cs.ensemble_tgv([((4, 32, 32), 0.1, 1000.0)]))
     with pytest.raises(cs.CSError, match="FP64"):
         cs.Ensemble([cs.tgv_config(None, dims=(32, 32, 32), precision=1)])
+
+
+def test_dependency_wait_timeout_returns_error_and_recovers(cuda):
+    """Failure detection without a fault: every dependency wait is made
+    unsatisfiable (it needs more finished items than the queue produces) and
+    limited to 64 polls.  The stage kernels give up, record the item, skip
+    the dependent items and return; the host sees CS_ERR_TIMEOUT.  With the
+    default restored the same ensemble steps correctly again."""
+    import torch
+    import compact_schemes_b200 as cs
+    boxes = BOXES[:2]
+    ens = cs.Ensemble(cs.ensemble_tgv(boxes))
+    q = _state(ens, boxes, 5)
+    ens.set_wait(64, 1 << 20)
+    ens.step(q)
+    with pytest.raises(cs.CSError, match="ran out") as ei:
+        ens.last_dt()
+    assert "-6" in str(ei.value)
+    ens.set_wait()
+    q = _state(ens, boxes, 5)
+    ref, dts = _per_box(boxes, q, ens, 2)
+    for _ in range(2):
+        ens.step(q)
+    assert ens.last_dt() == dts
+    for b in range(len(boxes)):
+        assert torch.equal(ens.box_view(q, b), ref[b]), b
+    ens.close()
