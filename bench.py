@@ -73,10 +73,11 @@ def mixed_512_gcbc_section(args, steps=6):
     n = 512
     lmx = n ** 3
     nbc = [[cs.BC_NON_REFLECTIVE, cs.BC_PERIODIC, cs.BC_PERIODIC]] * 2
+    from compact_schemes_b200.solver import REFINE_ALL
     out, states = {}, {}
-    for prec in (0, 1):
+    for prec in (0, 1, 2):  # plain, mixed, mixed with the refinement sweep
         s = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, nbc=nbc, gcbc=True,
-                                    precision=prec))
+                                    precision=min(prec, 1), refine=REFINE_ALL if prec == 2 else 0))
         q = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
         cs.tgv_init(q, (n, n, n), MACH, 1e-4, 0)
         choice = s.autotune(q, reps=1)
@@ -91,7 +92,13 @@ def mixed_512_gcbc_section(args, steps=6):
         out[prec] = {"ms_per_step": e0.elapsed_time(e1) / steps,
                      "schedule": {"%s_%s" % ("grad" if k == 0 else "flux", "xyz"[a]): v
                                   for (k, a), v in choice.items()}}
-        states[prec] = q
+        if prec < 2:
+            states[prec] = q
+        else:
+            d2 = [float((q[i * lmx:(i + 1) * lmx] - states[0][i * lmx:(i + 1) * lmx]).abs().max() /
+                        states[0][i * lmx:(i + 1) * lmx].abs().max()) for i in range(5)]
+            out[prec]["rel_err_vs_fp64_per_field"] = dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_E"], d2))
+            del q
         s.close()
     errs, errs_m = {}, {}
     mmax = max(float(states[0][i * lmx:(i + 1) * lmx].abs().max()) for i in (1, 2, 3))
@@ -108,6 +115,8 @@ def mixed_512_gcbc_section(args, steps=6):
             "plain": dict(out[0], value=rate(out[0]["ms_per_step"])),
             "mixed": dict(out[1], value=rate(out[1]["ms_per_step"])),
             "speedup_mixed_vs_plain": out[0]["ms_per_step"] / out[1]["ms_per_step"],
+            "mixed_refinement_sweep_on": dict(out[2], value=rate(out[2]["ms_per_step"]),
+                                              speedup_vs_plain=out[0]["ms_per_step"] / out[2]["ms_per_step"]),
             "rel_err_mixed_vs_fp64_per_field": errs,
             "rel_err_momentum_vs_max_momentum": errs_m, "steps_compared": steps + 1, "unit": UNIT}
 
@@ -911,8 +920,29 @@ def run_ours(args):
         errs_m = {n_: float((qm[i * lmx:(i + 1) * lmx] - qp[i * lmx:(i + 1) * lmx]).abs().max()) / mmax
                   for i, n_ in ((1, "rho_u"), (2, "rho_v"), (3, "rho_w"))}
         mvalue = world * pts_stages_per_step * args.steps / (tm_ms * 1e-3) / 1e6
+        # the same form with the FP64-residual refinement sweep after every FP32 solve
+        from compact_schemes_b200.solver import REFINE_ALL
+        sr = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, precision=1, refine=REFINE_ALL))
+        qr = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
+        cs.tgv_init(qr, dims, MACH, 1e-4, rank)
+        for _ in range(args.warmup):
+            sr.step(qr, 0.0)
+        barrier(world)
+        g0.record(stream)
+        for _ in range(args.steps):
+            sr.step(qr, 0.0)
+        g1.record(stream)
+        barrier(world)
+        tr_ms = max_over_ranks(g0.elapsed_time(g1), world)
+        errs_r = [float((qr[i * lmx:(i + 1) * lmx] - qp[i * lmx:(i + 1) * lmx]).abs().max() /
+                        qp[i * lmx:(i + 1) * lmx].abs().max()) for i in range(5)]
+        sr.close()
+        del qr
         mixed = {"value": mvalue, "unit": UNIT, "ms_per_step": tm_ms / args.steps,
                  "speedup_vs_plain": mvalue / value,
+                 "refinement_sweep_on": {"ms_per_step": tr_ms / args.steps, "speedup_vs_plain": t_ms / tr_ms,
+                                         "rel_err_vs_fp64_per_field":
+                                             dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_E"], errs_r))},
                  "rel_err_vs_fp64_per_field": dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_E"], errs)),
                  "rel_err_momentum_vs_max_momentum": errs_m,
                  "steps_compared": args.steps + args.warmup,

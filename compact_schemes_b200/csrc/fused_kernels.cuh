@@ -126,17 +126,29 @@ __device__ __forceinline__ double *field_line(double *sm, int field, int line) {
 
 // Solve the derivative of NF fields of this warp's line held in shared memory
 // and overwrite them with the result; G fields share one warp_solve call
-// (their table loads and shuffles are interleaved).
-template <int LT, int TL, int NF, int G = CSB_SOLVE_GROUP>
+// (their table loads and shuffles are interleaved).  ROWS: the single-rank
+// periodic closure rows of a group are formed on 8 lanes per line
+// (group_closure_rows) instead of serially by the owner lanes; bit-identical
+// either way, and faster only where registers allow it (measured: the
+// one-phase FP64 passes keep the serial form).
+template <int LT, int TL, int NF, int G = CSB_SOLVE_GROUP, bool ROWS = false>
 __device__ __forceinline__ void solve_fields(double *sm, int w, int lane, const DevTables<double> &tab,
                                              int nstart, int nend, const Coeffs &cf) {
 #pragma unroll 1
     for (int c0 = 0; c0 < NF; c0 += G) {
         double d[G][LT];
+        // single-rank periodic closures: the group's closure sums on 8 lanes per line
+        double *lines[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) lines[g] = field_line<LT, TL>(sm, c0 + g < NF ? c0 + g : c0, w);
+        const bool sums = ROWS && (nstart != 0 || nend != 0);
+        const double rows = sums ? group_closure_rows<LT, double, double, G>(lines, NF - c0, tab.n, lane, cf) : 0.0;
 #pragma unroll
         for (int g = 0; g < G; ++g) {
-            if (c0 + g < NF) deriv_rhs<LT, double, double>(field_line<LT, TL>(sm, c0 + g, w), tab.n, lane,
-                                                           nstart, nend, nullptr, cf, d[g]);
+            double own2[2];
+            if (sums) take_closure_rows(rows, g, lane, own2);
+            if (c0 + g < NF) deriv_rhs<LT, double, double>(lines[g], tab.n, lane, nstart, nend, nullptr, cf, d[g],
+                                                           sums ? own2 : nullptr);
             else {
 #pragma unroll
                 for (int t = 0; t < LT; ++t) d[g][t] = 0.0;

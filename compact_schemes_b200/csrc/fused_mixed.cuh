@@ -60,11 +60,16 @@ __device__ __forceinline__ void solve_lines_mx(float *const (&lines)[G], int nf,
     const int len = lane_len(lane, LT, tab.p, tab.last_len);
     // right-hand sides formed in FP64 (their differences cancel), rounded once
     float r32[G][LT], x[G][LT];
+    // single-rank periodic closures: the group's closure sums on 8 lanes per line
+    const bool sums = nstart != 0 || nend != 0;
+    const double rows = sums ? group_closure_rows<LT, double, float, G>(lines, nf, n, lane, cf) : 0.0;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
+        double own2[2];
+        if (sums) take_closure_rows(rows, g, lane, own2);
         if (g < nf) {
             double r64[LT];
-            deriv_rhs<LT, double, float>(lines[g], n, lane, nstart, nend, nullptr, cf, r64);
+            deriv_rhs<LT, double, float>(lines[g], n, lane, nstart, nend, nullptr, cf, r64, sums ? own2 : nullptr);
 #pragma unroll
             for (int t = 0; t < LT; ++t) x[g][t] = r32[g][t] = (float)r64[t];
         } else {

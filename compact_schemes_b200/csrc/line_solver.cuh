@@ -152,17 +152,69 @@ __device__ __forceinline__ CT get_at(const CT (&d)[LT], int t) {
     return r;
 }
 
+// One of the eight interface-closure sums of a line held in LineLayout<LT>
+// order in shared memory (single-rank periodic closure), summed in index
+// order k = 0..7 like the serial evaluation in deriv_rhs:
+//   d = 0 / 1: sum_k pbci[k] f[k] / pbci[8+k] f[k]           (rows 0 / 1, own end)
+//   d = 2 / 3: sum_k pbco[k] f[n-1-k] / pbco[8+k] f[n-1-k]   (rows 0 / 1, far end)
+//   d = 4 / 5: sum_k pbci[k] f[n-1-k] / pbci[8+k] f[n-1-k]   (rows n-1 / n-2, own end)
+//   d = 6 / 7: sum_k pbco[k] f[k] / pbco[8+k] f[k]           (rows n-1 / n-2, far end)
+template <int LT, typename CT, typename FT>
+__device__ __forceinline__ CT interface_sum(const FT *f, int n, int d, const Coeffs &cf) {
+    using L = LineLayout<LT>;
+    const bool bci = d < 2 || d == 4 || d == 5;
+    const bool asc = d < 2 || d >= 6;
+    const bool second = (d & 1) != 0;
+    CT s = CT(0);
+#pragma unroll
+    for (int k = 0; k < kLmd; ++k) {
+        const double c = bci ? (second ? cf.pbci[kLmd + k] : cf.pbci[k]) : (second ? cf.pbco[kLmd + k] : cf.pbco[k]);
+        s += xmul(CT(c), CT(f[L::pos(asc ? k : n - 1 - k)]));
+    }
+    return s;
+}
+
+// The closure rows of the single-rank periodic closure for a group of up to
+// four lines (lines[g], g < ng) solved together by one warp: lane 8g + d forms
+// interface_sum d of line g, so all 8 ng sums are formed at once instead of
+// one after another on the two owner lanes, then lanes 8g + {0, 1, 4, 5} add
+// the own-end and far-end sums of rows 0, 1, n-1, n-2 (the operations of the
+// serial evaluation, so the rows are bit-identical to it).  All 32 lanes must
+// call it.
+template <int LT, typename CT, typename FT, int G>
+__device__ __forceinline__ CT group_closure_rows(FT *const (&lines)[G], int ng, int n, int lane, const Coeffs &cf) {
+    static_assert(G <= 4, "eight lanes per line");
+    const int g = lane >> 3;
+    const FT *f = lines[0];
+#pragma unroll
+    for (int k = 1; k < G; ++k)
+        if (g == k) f = lines[k];
+    const CT dv = g < ng && g < G ? interface_sum<LT, CT, FT>(f, n, lane & 7, cf) : CT(0);
+    return dv + __shfl_down_sync(0xffffffffu, dv, 2);
+}
+// Rows of line g from group_closure_rows: lane 0 takes rows 0 and 1, every
+// other lane rows n-1 and n-2 (the owners of those rows are never lane 0 for
+// lines of 8 or more points).  All 32 lanes must call it.
+template <typename CT>
+__device__ __forceinline__ void take_closure_rows(CT x, int g, int lane, CT (&own2)[2]) {
+    const int src = 8 * g + (lane == 0 ? 0 : 4);
+    own2[0] = __shfl_sync(0xffffffffu, x, src);
+    own2[1] = __shfl_sync(0xffffffffu, x, src + 1);
+}
+
 // Right-hand side of the compact derivative for the rows of this lane,
 // restating build_system (src/cuda/kernels/numerics_device_pc.hpp:176-293):
 // interior aa*(f[j+1]-f[j-1]) + bb*(f[j+2]-f[j-2]); physical closure rows
 // (ndf = 0) or interface closure rows (ndf = 1: 8-point pbci sums plus the
 // received pbco sums; `recv4` = {row0, row1, row n-1, row n-2} received
-// values, or the line's own far-end sums for single-rank periodic).
+// values, or the line's own far-end sums for single-rank periodic; `own2`,
+// when given for that case, holds the line's closure rows already summed by
+// group_closure_rows / take_closure_rows).
 // `f` is the line in LineLayout<LT> order in shared memory.
 template <int LT, typename CT, typename FT>
 __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nstart, int nend,
                                           const CT *recv4_or_null, const Coeffs &cf,
-                                          CT (&d)[LT]) {
+                                          CT (&d)[LT], const CT *own2 = nullptr) {
     using L = LineLayout<LT>;
     const int j0 = lane * LT;
     CT w[LT + 4];
@@ -185,6 +237,9 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
             if (nstart == 0) {
                 d[0] = xmul(CT(kAb00), f0) + xmul(CT(kAb01), f1) + xmul(CT(kAb02), f2);
                 d[1] = xmul(CT(kAb10), f2 - f0);
+            } else if (own2 && !recv4_or_null) {
+                d[0] = own2[0];
+                d[1] = own2[1];
             } else {
                 CT r0, r1;
                 if (recv4_or_null) {
@@ -213,6 +268,9 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
             if (nend == 0) {
                 e1 = -(xmul(CT(kAb00), g0) + xmul(CT(kAb01), g1) + xmul(CT(kAb02), g2));
                 e2 = xmul(-CT(kAb10), g2 - g0);
+            } else if (own2 && !recv4_or_null) {
+                e1 = -own2[0];
+                e2 = -own2[1];
             } else {
                 CT r2, r3;
                 if (recv4_or_null) {

@@ -66,15 +66,24 @@ __device__ __forceinline__ void run_pipeline(int64_t ntiles, Stage &&stage, Stor
     }
 }
 
-// Solve fields c0 .. c0+G-1 (< NF) of one line of an FP64 tile in place.
-template <int LT, int TL, int G>
+// Solve fields c0 .. c0+G-1 (< NF) of one line of an FP64 tile in place;
+// ROWS as in solve_fields (the TMA gradient pass forms its closure rows on 8
+// lanes per line, measured faster there).
+template <int LT, int TL, int G, bool ROWS = false>
 __device__ __forceinline__ void solve_group(double *sm, int line, int c0, int nf, int lane,
                                             const DevTables<double> &tab, int nstart, int nend, const Coeffs &cf) {
     double d[G][LT];
+    double *lines[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) lines[g] = field_line<LT, TL>(sm, c0 + g < nf ? c0 + g : c0, line);
+    const bool sums = ROWS && (nstart != 0 || nend != 0);
+    const double rows = sums ? group_closure_rows<LT, double, double, G>(lines, nf - c0, tab.n, lane, cf) : 0.0;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
-        if (c0 + g < nf) deriv_rhs<LT, double, double>(field_line<LT, TL>(sm, c0 + g, line), tab.n, lane, nstart,
-                                                       nend, nullptr, cf, d[g]);
+        double own2[2];
+        if (sums) take_closure_rows(rows, g, lane, own2);
+        if (c0 + g < nf) deriv_rhs<LT, double, double>(lines[g], tab.n, lane, nstart, nend, nullptr, cf, d[g],
+                                                       sums ? own2 : nullptr);
         else {
 #pragma unroll
             for (int t = 0; t < LT; ++t) d[g][t] = 0.0;

@@ -236,7 +236,7 @@ k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, Dev
             int64_t base, stride;
             const int l = w % TL;
             if (tma_line<AXIS, TL>(t, l, geo, lxi, let, F, base, stride))
-                solve_group<LT, TL, FPW>(solve, l, (w / TL) * FPW, 4, lane, tab, nstart, nend, cf);
+                solve_group<LT, TL, FPW, true>(solve, l, (w / TL) * FPW, 4, lane, tab, nstart, nend, cf);
         }
         __syncthreads();
         tma_points<AXIS, TL>(n, [&](int l, int j) {

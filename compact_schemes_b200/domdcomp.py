@@ -19,6 +19,8 @@ a single GPU.
 """
 from __future__ import annotations
 
+import weakref
+
 from . import BC_INTER_SUBDOMAINS, BC_PERIODIC
 
 
@@ -151,7 +153,10 @@ def exchange(send, recv, dd, nn, group=None):
             part(recv, ip_recv).copy_(landing)
 
 
-_P2P_READY = set()
+# process groups whose first point-to-point batch has been preceded by a
+# barrier; weak references, so a destroyed group (and a new one created in
+# its place, possibly at the same address) is never mistaken for a ready one
+_P2P_READY = weakref.WeakSet()
 
 
 def mpigo(numerics, dd, variable_id, group=None):
@@ -161,7 +166,7 @@ def mpigo(numerics, dd, variable_id, group=None):
     rank of the group calls it, in the same order of variables."""
     import torch
     import torch.distributed as dist
-    key = id(group)
+    key = group if group is not None else dist.group.WORLD
     if key not in _P2P_READY:
         # the first point-to-point batch of an NCCL group must involve every
         # rank; a barrier on the group first makes any later subset valid
