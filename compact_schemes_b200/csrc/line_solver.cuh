@@ -217,12 +217,17 @@ __device__ __forceinline__ void deriv_rhs(const FT *f, int n, int lane, int nsta
                                           CT (&d)[LT], const CT *own2 = nullptr) {
     using L = LineLayout<LT>;
     const int j0 = lane * LT;
+    // points j0-2 .. j0+LT+1: the last two of the previous lane's chunk, this
+    // lane's chunk and the first two of the next lane's (compile-time slots,
+    // no clamping).  Outside 0..n-1 the slot positions wrap inside the line's
+    // slot and hold unused values: only rows 0, 1, n-2, n-1 reach there, and
+    // the owner lanes rebuild those rows below.
     CT w[LT + 4];
 #pragma unroll
     for (int k = 0; k < LT + 4; ++k) {
-        int j = j0 + k - 2;
-        j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
-        w[k] = CT(f[L::pos(j)]);
+        const int t = (k + LT - 2) % LT;
+        const int dc = k < 2 ? -1 : (k >= LT + 2 ? 1 : 0);
+        w[k] = CT(f[L::pos_ct(lane + dc, t)]);
     }
 #pragma unroll
     for (int t = 0; t < LT; ++t)
