@@ -12,12 +12,12 @@ namespace csb {
 bool tma_grad_geometry(int axis, const cs_dcomp &d, int lt, int smem_max, TmaGeom &g, size_t &smem_bytes) {
     const int n = axis == 0 ? d.lxi : (axis == 1 ? d.let : d.lze);
     if (n > 512 || lt > 16) return false;
-    const int tl = lt <= 8 ? 8 : 4;
+    const int tl = kTmaTile;
     // row strides of the tensor maps are multiples of 16 bytes
     if (axis < 2 ? (d.lxi % 2) : (((int64_t)d.lxi * d.let) % 2)) return false;
     g.nbox = n > 256 ? 2 : 1;
     const int per = (n + g.nbox - 1) / g.nbox;
-    g.boxlen = (per + 3) / 4 * 4;  // 128-byte aligned boxes in shared memory
+    g.boxlen = (per + 3) / 4 * 4;  // boxes of 5 x 4 x boxlen doubles: 128-byte aligned in shared memory
     if (g.boxlen > 256) return false;
     const int64_t F = axis == 0 ? (int64_t)d.let * d.lze : (axis == 1 ? (int64_t)d.lxi * d.lze : (int64_t)d.lxi * d.let);
     g.tiles_x = (d.lxi + tl - 1) / tl;
@@ -28,8 +28,8 @@ bool tma_grad_geometry(int axis, const cs_dcomp &d, int lt, int smem_max, TmaGeo
     g.tile_bytes = (unsigned)stage;
     const size_t slot = (size_t)32 * lt + 1;
     // two staging buffers, the line-solver layout of 4 fields, two mbarriers,
-    // and up to 1024 bytes to align the staging buffers
-    smem_bytes = 2 * stage + (size_t)4 * tl * slot * sizeof(double) + 2 * sizeof(uint64_t) + 1024;
+    // and up to 128 bytes to align the staging buffers
+    smem_bytes = 2 * stage + (size_t)4 * tl * slot * sizeof(double) + 2 * sizeof(uint64_t) + 128;
     return smem_bytes <= (size_t)smem_max;
 }
 

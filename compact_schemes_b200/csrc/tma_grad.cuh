@@ -1,24 +1,26 @@
 // tma_grad.cuh -- gradient pass with pencils staged into shared memory by TMA.
 //
-// Persistent CTAs (one per SM, 16 warps) walk the tiles t_k = blockIdx.x +
-// k * gridDim.x of a gradient pass.  A tile is TL lines of the state q along
-// AXIS; one thread issues it as tensor copies (cp.async.bulk.tensor, no
-// multicast) of all five conserved fields into one of two staging buffers,
-// completing on that buffer's mbarrier, two tiles ahead of the tile being
-// solved.  The y and z pencils are boxes of TL consecutive x (or x-y)
-// positions by the whole line, so the strided lines arrive as dense rows of
-// 64 bytes; the x pencils are TL consecutive rows.  Per tile:
+// Persistent CTAs walk the tiles t_k = blockIdx.x + k * gridDim.x of a
+// gradient pass: two 256-thread CTAs per SM for lines of up to 256 points,
+// one 512-thread CTA for lines of 257-512 points.  A tile is TL = 4 lines of
+// the state q along AXIS; one thread issues it as tensor copies
+// (cp.async.bulk.tensor, no multicast) of all five conserved fields into one
+// of two staging buffers, completing on that buffer's mbarrier, two tiles
+// ahead of the tile being solved.  The y and z pencils are boxes of TL
+// consecutive x (or x-y) positions by the whole line, so the strided lines
+// arrive as dense rows; the x pencils are TL consecutive rows.  Per tile:
 //   1. wait for the staging buffer (bounded);
 //   2. every thread reads its points of the staged q, forms the primitives
 //      (u, v, w, T) and writes them into the line-solver layout (the staged
 //      rows are read along the tile's x, the transposition into lines happens
 //      here), and reduces the CFL maxima when asked;
 //   3. one thread refills the staging buffer with tile k + 2;
-//   4. warp w solves fields 2 (w / TL) .. +1 (TL = 8) or field w / TL
-//      (TL = 4) of line w % TL in place;
+//   4. each warp solves two fields (one for 512-point lines) of one line in
+//      place;
 //   5. the four derivatives go to HBM with coalesced stores.
-// So the HBM reads of two tiles are in flight while a tile is formed, solved
-// and stored, with no per-element address arithmetic on the load side.  The
+// The HBM reads of two tiles are in flight while a tile is formed, solved
+// and stored, with no per-element address arithmetic on the load side, and
+// with two CTAs per SM one CTA's solve overlaps the other's stores.  The
 // arithmetic is that of k_grad (same primitives, same right-hand sides, same
 // warp solves and field grouping): results are bit-identical to it.
 //
@@ -34,8 +36,6 @@
 
 namespace csb {
 
-constexpr int kTmaThreads = 512;
-constexpr int kTmaWarps = kTmaThreads / 32;
 // iterations of a bounded mbarrier wait (each try_wait suspends for a
 // hardware-chosen time; with the backoff below the limit is well over 1 s)
 constexpr unsigned kTmaWaitLimit = 1u << 22;
@@ -93,10 +93,14 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
-// Lines per tile of the TMA gradient pass for chunk length LT.
+// Tiles of the TMA gradient pass: 4 lines.  Lines of up to 256 points run
+// 256-thread CTAs, two per SM (each 113 KB of shared memory), so that one CTA
+// solves while the other stages and stores; lines of 257-512 points run one
+// 512-thread CTA per SM.
+constexpr int kTmaTile = 4;
 template <int LT>
-constexpr int tma_tile() {
-    return LT <= 8 ? 8 : 4;
+constexpr int tma_threads() {
+    return LT <= 8 ? 256 : 512;
 }
 
 // Staged offset of field f, tile line l, line point j (box b = j / boxlen).
@@ -147,34 +151,35 @@ __device__ __forceinline__ bool tma_line(int t, int l, const TmaGeom &g, int lxi
     return fidx < F;
 }
 
-// Points (l, j) of a tile owned by this thread: x tiles give each line
-// kTmaWarps / TL warps walking it with lane-consecutive j; y/z tiles give
-// thread t line t % TL and rows t / TL + (kTmaThreads / TL) k.
-template <int AXIS, int TL, typename Fn>
+// Points (l, j) of a tile owned by this thread (NT threads): x tiles give
+// each line NT / 32 / TL warps walking it with lane-consecutive j; y/z tiles
+// give thread t line t % TL and rows t / TL + (NT / TL) k.
+template <int AXIS, int TL, int NT, typename Fn>
 __device__ __forceinline__ void tma_points(int n, Fn &&fn) {
     const int tid = threadIdx.x;
     if (AXIS == 0) {
-        constexpr int WPL = kTmaWarps / TL;
+        constexpr int WPL = NT / 32 / TL;
         const int w = tid >> 5, l = w % TL;
         for (int j = (w / TL) * 32 + (tid & 31); j < n; j += 32 * WPL) fn(l, j);
     } else {
         const int l = tid % TL;
-        for (int j = tid / TL; j < n; j += kTmaThreads / TL) fn(l, j);
+        for (int j = tid / TL; j < n; j += NT / TL) fn(l, j);
     }
 }
 
 template <int LT, int AXIS, bool DTRED>
-__global__ void __launch_bounds__(kTmaThreads, 1)
+__global__ void __launch_bounds__(tma_threads<LT>(), LT <= 8 ? 2 : 1)
 k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, DevTables<double> tab, TmaGeom geo,
            int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf, Phys ph,
            unsigned long long *__restrict__ dtacc, int *__restrict__ err) {
-    constexpr int TL = tma_tile<LT>();
-    constexpr int FPW = 4 * TL / kTmaWarps;  // fields per warp solve
+    constexpr int TL = kTmaTile;
+    constexpr int NT = tma_threads<LT>();
+    constexpr int FPW = 4 * TL / (NT / 32);  // fields per warp solve
     using L = LineLayout<LT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int stage_elems = geo.nbox * 5 * TL * geo.boxlen;
-    // staging boxes start on 1024-byte boundaries (the launch adds the slack)
-    double *stage0 = reinterpret_cast<double *>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
+    // staging boxes start on 128-byte boundaries (the launch adds the slack)
+    double *stage0 = reinterpret_cast<double *>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
     double *solve = stage0 + 2 * stage_elems;
     uint64_t *bars = reinterpret_cast<uint64_t *>(solve + 4 * TL * L::kSlot);
     const int n = tab.n;
@@ -205,7 +210,7 @@ k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, Dev
             return;
         }
         // primitives into the line layout
-        tma_points<AXIS, TL>(n, [&](int l, int j) {
+        tma_points<AXIS, TL, NT>(n, [&](int l, int j) {
             int64_t base, stride;
             if (!tma_line<AXIS, TL>(t, l, geo, lxi, let, F, base, stride)) return;
             const Prim s = primitives(stg[tma_staged<AXIS, TL>(0, l, j, geo)], stg[tma_staged<AXIS, TL>(1, l, j, geo)],
@@ -239,7 +244,7 @@ k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, Dev
                 solve_group<LT, TL, FPW, true>(solve, l, (w / TL) * FPW, 4, lane, tab, nstart, nend, cf);
         }
         __syncthreads();
-        tma_points<AXIS, TL>(n, [&](int l, int j) {
+        tma_points<AXIS, TL, NT>(n, [&](int l, int j) {
             int64_t base, stride;
             if (!tma_line<AXIS, TL>(t, l, geo, lxi, let, F, base, stride)) return;
             const int64_t gi = base + j * stride;
@@ -277,8 +282,11 @@ int launch_grad_tma_t(const PassArgs &a, const cs_dcomp &d, const double *q, boo
     if (int rc = tma_grad_map(AXIS, d, geo, q, map)) return rc;
     auto kern = dtred ? k_grad_tma<LT, AXIS, true> : k_grad_tma<LT, AXIS, false>;
     if (int rc = set_smem(kern, smem)) return rc;
-    const int blocks = geo.ntiles < a.nsm ? geo.ntiles : a.nsm;
-    kern<<<blocks, kTmaThreads, smem, st>>>(map, a.grad + (int64_t)AXIS * 4 * a.lmx, a.tab->t64, geo, a.lxi, a.let,
+    int per = 0;
+    CSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, tma_threads<LT>(), smem));
+    if (per < 1) return set_error(CS_ERR_UNSUPPORTED, "TMA gradient pass: a CTA does not fit an SM");
+    const int blocks = geo.ntiles < a.nsm * per ? geo.ntiles : a.nsm * per;
+    kern<<<blocks, tma_threads<LT>(), smem, st>>>(map, a.grad + (int64_t)AXIS * 4 * a.lmx, a.tab->t64, geo, a.lxi, a.let,
                                             a.lmx, a.F, a.nstart, a.nend, a.cf, a.ph, a.dtacc, err);
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
