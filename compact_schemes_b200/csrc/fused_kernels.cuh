@@ -252,22 +252,14 @@ enum FluxMode { kWrite = 0, kAccum = 1, kAccumRk = 2, kWriteRk = 3 };
 
 // Flux components F[m][AXIS] at one point from the state and the gradients
 // (calc_fluxes_pre_compute_kernel<Visc>, src/cuda/kernels/physics.hpp:42-193,
-// with tau / heat flux of calc_viscous_shear_stress_final_kernel, :285-333).
-// CG: the gradients were written earlier in the same launch by other CTAs
-// (ensemble launch) and are read from L2 (ld.global.cg).
-template <int AXIS, bool VISC, bool CG = false, bool FM = false>
-__device__ __forceinline__ void point_flux(const double *__restrict__ q, const double *__restrict__ g,
-                                           int64_t lmx, int64_t gi, const Phys &ph, double (&fl)[5],
-                                           const FieldMet &fm = FieldMet{}) {
-    const double q0 = __ldg(q + gi), q1 = __ldg(q + lmx + gi), q2 = __ldg(q + 2 * lmx + gi);
-    const double q3 = __ldg(q + 3 * lmx + gi), q4 = __ldg(q + 4 * lmx + gi);
-    double gr[12];
-    if (VISC) {
-#pragma unroll
-        for (int k = 0; k < 12; ++k) gr[k] = CG ? __ldcg(g + k * lmx + gi) : __ldg(g + k * lmx + gi);
-    }
+// with tau / heat flux of calc_viscous_shear_stress_final_kernel, :285-333),
+// from the point's values: state q0..q4, gradients gr[12] (G[b][c] at
+// 4 b + c) and metrics pm.
+template <int AXIS, bool VISC>
+__device__ __forceinline__ void flux_values(double q0, double q1, double q2, double q3, double q4,
+                                            const double (&gr)[12], const PointMet &pm, const Phys &ph,
+                                            double (&fl)[5]) {
     const Prim s = primitives(q0, q1, q2, q3, q4);
-    const PointMet pm = point_met<FM>(ph, fm, lmx, gi);
     const double *Ma = pm.M[AXIS];
     const double ss = xmul(Ma[0], s.u + ph.umf[0]) + xmul(Ma[1], s.v + ph.umf[1]) + xmul(Ma[2], s.w + ph.umf[2]);
     fl[0] = xmul(q0, ss);
@@ -301,6 +293,24 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
         fl[3] -= xmul(Ma[0], tzx) + xmul(Ma[1], tyz) + xmul(Ma[2], tzz);
         fl[4] -= xmul(Ma[0], hx) + xmul(Ma[1], hy) + xmul(Ma[2], hz);
     }
+}
+
+// The same loading the point's values from HBM.  CG: the gradients were
+// written earlier in the same launch by other CTAs (ensemble launch) and are
+// read from L2 (ld.global.cg).
+template <int AXIS, bool VISC, bool CG = false, bool FM = false>
+__device__ __forceinline__ void point_flux(const double *__restrict__ q, const double *__restrict__ g,
+                                           int64_t lmx, int64_t gi, const Phys &ph, double (&fl)[5],
+                                           const FieldMet &fm = FieldMet{}) {
+    const double q0 = __ldg(q + gi), q1 = __ldg(q + lmx + gi), q2 = __ldg(q + 2 * lmx + gi);
+    const double q3 = __ldg(q + 3 * lmx + gi), q4 = __ldg(q + 4 * lmx + gi);
+    double gr[12];
+    if (VISC) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gr[k] = CG ? __ldcg(g + k * lmx + gi) : __ldg(g + k * lmx + gi);
+    }
+    const PointMet pm = point_met<FM>(ph, fm, lmx, gi);
+    flux_values<AXIS, VISC>(q0, q1, q2, q3, q4, gr, pm, ph, fl);
 }
 
 // One tile of the flux pass (TL * 32 threads; sm holds 5 * TL line slots).

@@ -46,36 +46,39 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-int tma_grad_map(int axis, const cs_dcomp &d, const TmaGeom &g, const double *q, CUtensorMap &map) {
+int tma_field_map(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const double *base, CUtensorMap &map) {
     auto fn = encode_fn();
     if (!fn) return set_error(CS_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-    if (reinterpret_cast<uintptr_t>(q) % 16) return set_error(CS_ERR_INVALID, "TMA gradient pass: q not 16-byte aligned");
-    const int tl = g.tile_bytes / (g.nbox * 5 * g.boxlen * sizeof(double));
+    if (reinterpret_cast<uintptr_t>(base) % 16) return set_error(CS_ERR_INVALID, "TMA pass: field block not 16-byte aligned");
     const cuuint64_t E = sizeof(double), lmx = (cuuint64_t)d.lmx;
     cuuint64_t dims[4], strides[3];
     cuuint32_t box[4], estr[4] = {1, 1, 1, 1};
     cuuint32_t rank;
     if (axis == 0) {
         rank = 3;
-        dims[0] = d.lxi; dims[1] = (cuuint64_t)d.let * d.lze; dims[2] = 5;
+        dims[0] = d.lxi; dims[1] = (cuuint64_t)d.let * d.lze; dims[2] = nf;
         strides[0] = d.lxi * E; strides[1] = lmx * E;
-        box[0] = g.boxlen; box[1] = tl; box[2] = 5;
+        box[0] = boxlen; box[1] = tl; box[2] = nf;
     } else if (axis == 1) {
         rank = 4;
-        dims[0] = d.lxi; dims[1] = d.let; dims[2] = d.lze; dims[3] = 5;
+        dims[0] = d.lxi; dims[1] = d.let; dims[2] = d.lze; dims[3] = nf;
         strides[0] = d.lxi * E; strides[1] = (cuuint64_t)d.lxi * d.let * E; strides[2] = lmx * E;
-        box[0] = tl; box[1] = g.boxlen; box[2] = 1; box[3] = 5;
+        box[0] = tl; box[1] = boxlen; box[2] = 1; box[3] = nf;
     } else {
         rank = 3;
-        dims[0] = (cuuint64_t)d.lxi * d.let; dims[1] = d.lze; dims[2] = 5;
+        dims[0] = (cuuint64_t)d.lxi * d.let; dims[1] = d.lze; dims[2] = nf;
         strides[0] = (cuuint64_t)d.lxi * d.let * E; strides[1] = lmx * E;
-        box[0] = tl; box[1] = g.boxlen; box[2] = 5;
+        box[0] = tl; box[1] = boxlen; box[2] = nf;
     }
-    CUresult r = fn(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, const_cast<double *>(q), dims, strides, box, estr,
+    CUresult r = fn(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, const_cast<double *>(base), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(CS_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return CS_OK;
+}
+
+int tma_grad_map(int axis, const cs_dcomp &d, const TmaGeom &g, const double *q, CUtensorMap &map) {
+    return tma_field_map(axis, d, kTmaTile, g.boxlen, 5, q, map);
 }
 
 }  // namespace csb

@@ -270,6 +270,9 @@ k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, Dev
 // Host side (tma_grad.cu).
 // Encode the tensor map of q [5][lmx] for a gradient pass along `axis`.
 int tma_grad_map(int axis, const cs_dcomp &d, const TmaGeom &g, const double *q, CUtensorMap &map);
+// Tensor map over nf consecutive fields [nf][lmx] starting at base, boxes of
+// tl lines by boxlen points along `axis` by nf fields.
+int tma_field_map(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const double *base, CUtensorMap &map);
 
 template <int LT, int AXIS>
 int launch_grad_tma_t(const PassArgs &a, const cs_dcomp &d, const double *q, bool dtred, int *err,
