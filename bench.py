@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--no-config1", action="store_true")
     p.add_argument("--no-dropin", action="store_true")
     p.add_argument("--no-filter", action="store_true")
+    p.add_argument("--schedule", default="auto", choices=["auto", "tma", "onephase"],
+                   help="auto: the autotuner picks each pass's schedule (default); tma / onephase: fixed, no "
+                        "autotuning (used for ncu launch lists, where the autotuner's own timings are distorted)")
     return p.parse_args()
 
 
@@ -809,13 +812,16 @@ def run_ours(args):
     dims = (n, n, n)
     lmx = n ** 3
     pts_stages_per_step = lmx * 4
-    cfg = cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True)
+    from compact_schemes_b200.solver import SCHED_AUTO, SCHED_ONEPHASE, SCHED_TMA
+    sched = {"auto": SCHED_AUTO, "tma": SCHED_TMA, "onephase": SCHED_ONEPHASE}[args.schedule]
+    cfg = cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, schedule=sched)
     s = cs.Solver(cfg)
     q = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
     cs.tgv_init(q, dims, MACH, 1e-4, rank)
     stream = torch.cuda.current_stream()
 
-    tuned = s.autotune(q, reps=1)  # per-pass schedule; the state is not modified
+    # per-pass schedule (the state is not modified)
+    tuned = s.autotune(q, reps=1) if args.schedule == "auto" else s.schedule()
     for _ in range(args.warmup):
         s.step(q, 0.0)
     barrier(world)

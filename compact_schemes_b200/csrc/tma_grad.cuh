@@ -103,19 +103,6 @@ constexpr int tma_threads() {
     return LT <= 8 ? 256 : 512;
 }
 
-// Staged offset of field f, tile line l, line point j (box b = j / boxlen).
-template <int AXIS, int TL>
-__device__ __forceinline__ int tma_staged(int f, int l, int j, const TmaGeom &g) {
-    int b = 0, jj = j;
-    while (jj >= g.boxlen) {
-        jj -= g.boxlen;
-        ++b;
-    }
-    const int box = b * 5 * TL * g.boxlen;
-    if (AXIS == 0) return box + (f * TL + l) * g.boxlen + jj;
-    return box + (f * g.boxlen + jj) * TL + l;
-}
-
 // Issue the copies of tile t into the staging buffer dst (one thread).
 template <int AXIS, int TL>
 __device__ __forceinline__ void tma_issue_tile(double *dst, const CUtensorMap *map, int t, const TmaGeom &g,
@@ -149,22 +136,6 @@ __device__ __forceinline__ bool tma_line(int t, int l, const TmaGeom &g, int lxi
     base = fidx;
     stride = (int64_t)lxi * let;
     return fidx < F;
-}
-
-// Points (l, j) of a tile owned by this thread (NT threads): x tiles give
-// each line NT / 32 / TL warps walking it with lane-consecutive j; y/z tiles
-// give thread t line t % TL and rows t / TL + (NT / TL) k.
-template <int AXIS, int TL, int NT, typename Fn>
-__device__ __forceinline__ void tma_points(int n, Fn &&fn) {
-    const int tid = threadIdx.x;
-    if (AXIS == 0) {
-        constexpr int WPL = NT / 32 / TL;
-        const int w = tid >> 5, l = w % TL;
-        for (int j = (w / TL) * 32 + (tid & 31); j < n; j += 32 * WPL) fn(l, j);
-    } else {
-        const int l = tid % TL;
-        for (int j = tid / TL; j < n; j += NT / TL) fn(l, j);
-    }
 }
 
 template <int LT, int AXIS, bool DTRED>
@@ -209,32 +180,42 @@ k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, Dev
             }
             return;
         }
+        // this thread's line of the tile (fixed per thread) and where it lives
+        // in HBM and in the staging buffer
+        const int ml = AXIS == 0 ? w % TL : tid % TL;
+        const int mj0 = AXIS == 0 ? (w / TL) * 32 + lane : tid / TL;
+        constexpr int MDJ = AXIS == 0 ? 32 * (NT / 32 / TL) : NT / TL;
+        int64_t mbase, mstride;
+        const bool mvalid = tma_line<AXIS, TL>(t, ml, geo, lxi, let, F, mbase, mstride);
+        const int fstride = AXIS == 0 ? TL * geo.boxlen : geo.boxlen * TL;  // between staged fields
+        const int box_elems = 5 * TL * geo.boxlen;
         // primitives into the line layout
-        tma_points<AXIS, TL, NT>(n, [&](int l, int j) {
-            int64_t base, stride;
-            if (!tma_line<AXIS, TL>(t, l, geo, lxi, let, F, base, stride)) return;
-            const Prim s = primitives(stg[tma_staged<AXIS, TL>(0, l, j, geo)], stg[tma_staged<AXIS, TL>(1, l, j, geo)],
-                                      stg[tma_staged<AXIS, TL>(2, l, j, geo)], stg[tma_staged<AXIS, TL>(3, l, j, geo)],
-                                      stg[tma_staged<AXIS, TL>(4, l, j, geo)]);
-            const int pj = L::pos(j);
-            field_line<LT, TL>(solve, 0, l)[pj] = s.u;
-            field_line<LT, TL>(solve, 1, l)[pj] = s.v;
-            field_line<LT, TL>(solve, 2, l)[pj] = s.w;
-            field_line<LT, TL>(solve, 3, l)[pj] = s.T;
-            if (DTRED) {
-                // calc_time_step_kernel (src/cuda/kernels/physics.hpp:335-427), uniform metrics
-                const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
-                double rr2 = 0.0;
+        if (mvalid) {
+            for (int j = mj0; j < n; j += MDJ) {
+                const int bx = j >= geo.boxlen ? 1 : 0, jj = j - bx * geo.boxlen;
+                const int o = bx * box_elems + (AXIS == 0 ? ml * geo.boxlen + jj : jj * TL + ml);
+                const Prim s = primitives(stg[o], stg[o + fstride], stg[o + 2 * fstride], stg[o + 3 * fstride],
+                                          stg[o + 4 * fstride]);
+                const int pj = L::pos(j);
+                field_line<LT, TL>(solve, 0, ml)[pj] = s.u;
+                field_line<LT, TL>(solve, 1, ml)[pj] = s.v;
+                field_line<LT, TL>(solve, 2, ml)[pj] = s.w;
+                field_line<LT, TL>(solve, 3, ml)[pj] = s.T;
+                if (DTRED) {
+                    // calc_time_step_kernel (src/cuda/kernels/physics.hpp:335-427), uniform metrics
+                    const double uu = s.u + ph.umf[0], vv = s.v + ph.umf[1], ww = s.w + ph.umf[2];
+                    double rr2 = 0.0;
 #pragma unroll
-                for (int a = 0; a < 3; ++a)
-                    rr2 += fabs(xmul(ph.M[a][0], uu) + xmul(ph.M[a][1], vv) + xmul(ph.M[a][2], ww));
-                const double ssi = fabs(ph.J);
-                const double v1 = xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi);
-                const double v2 = s.ri * ph.mu * ph.rr1 * ssi * ssi;
-                m1 = fmax(m1, v1);
-                m2 = fmax(m2, v2);
+                    for (int a = 0; a < 3; ++a)
+                        rr2 += fabs(xmul(ph.M[a][0], uu) + xmul(ph.M[a][1], vv) + xmul(ph.M[a][2], ww));
+                    const double ssi = fabs(ph.J);
+                    const double v1 = xmul(sqrt(xmul(s.T, ph.rr1)) + rr2, ssi);
+                    const double v2 = s.ri * ph.mu * ph.rr1 * ssi * ssi;
+                    m1 = fmax(m1, v1);
+                    m2 = fmax(m2, v2);
+                }
             }
-        });
+        }
         __syncthreads();
         if (tid == 0 && k + 2 < K) tma_issue_tile<AXIS, TL>(stg, &qmap, t + 2 * G, geo, &bars[b]);
         {
@@ -244,14 +225,14 @@ k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, Dev
                 solve_group<LT, TL, FPW, true>(solve, l, (w / TL) * FPW, 4, lane, tab, nstart, nend, cf);
         }
         __syncthreads();
-        tma_points<AXIS, TL, NT>(n, [&](int l, int j) {
-            int64_t base, stride;
-            if (!tma_line<AXIS, TL>(t, l, geo, lxi, let, F, base, stride)) return;
-            const int64_t gi = base + j * stride;
-            const int pj = L::pos(j);
+        if (mvalid) {
+            for (int j = mj0; j < n; j += MDJ) {
+                const int64_t gi = mbase + j * mstride;
+                const int pj = L::pos(j);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) g[c * lmx + gi] = field_line<LT, TL>(solve, c, l)[pj];
-        });
+                for (int c = 0; c < 4; ++c) g[c * lmx + gi] = field_line<LT, TL>(solve, c, ml)[pj];
+            }
+        }
         __syncthreads();
     }
     if (DTRED) {
