@@ -254,20 +254,35 @@ enum FluxMode { kWrite = 0, kAccum = 1, kAccumRk = 2, kWriteRk = 3 };
 // (calc_fluxes_pre_compute_kernel<Visc>, src/cuda/kernels/physics.hpp:42-193,
 // with tau / heat flux of calc_viscous_shear_stress_final_kernel, :285-333),
 // from the point's values: state q0..q4, gradients gr[12] (G[b][c] at
-// 4 b + c) and metrics pm.
-template <int AXIS, bool VISC>
+// 4 b + c) and metrics pm.  DIAG: the metric matrix is diagonal (the uniform
+// Cartesian grid, M[b][k] = 0 for b != k), and the products with its zero
+// entries are left out: each sum then adds the same nonzero terms in the same
+// order, so the result equals the full evaluation's (up to the sign of an
+// exactly zero value).
+template <int AXIS, bool VISC, bool DIAG = false>
 __device__ __forceinline__ void flux_values(double q0, double q1, double q2, double q3, double q4,
                                             const double (&gr)[12], const PointMet &pm, const Phys &ph,
                                             double (&fl)[5]) {
     const Prim s = primitives(q0, q1, q2, q3, q4);
     const double *Ma = pm.M[AXIS];
-    const double ss = xmul(Ma[0], s.u + ph.umf[0]) + xmul(Ma[1], s.v + ph.umf[1]) + xmul(Ma[2], s.w + ph.umf[2]);
+    const double vel[3] = {s.u, s.v, s.w};
+    double ss;
+    if (DIAG) ss = xmul(Ma[AXIS], vel[AXIS] + ph.umf[AXIS]);
+    else ss = xmul(Ma[0], s.u + ph.umf[0]) + xmul(Ma[1], s.v + ph.umf[1]) + xmul(Ma[2], s.w + ph.umf[2]);
     fl[0] = xmul(q0, ss);
-    fl[1] = xmul(q1, ss) + xmul(Ma[0], s.p);
-    fl[2] = xmul(q2, ss) + xmul(Ma[1], s.p);
-    fl[3] = xmul(q3, ss) + xmul(Ma[2], s.p);
-    fl[4] = xmul(q4 + s.p, ss) -
-            xmul(s.p, xmul(ph.umf[0], Ma[0]) + xmul(ph.umf[1], Ma[1]) + xmul(ph.umf[2], Ma[2]));
+    if (DIAG) {
+        fl[1] = xmul(q1, ss);
+        fl[2] = xmul(q2, ss);
+        fl[3] = xmul(q3, ss);
+        fl[1 + AXIS] += xmul(Ma[AXIS], s.p);
+        fl[4] = xmul(q4 + s.p, ss) - xmul(s.p, xmul(ph.umf[AXIS], Ma[AXIS]));
+    } else {
+        fl[1] = xmul(q1, ss) + xmul(Ma[0], s.p);
+        fl[2] = xmul(q2, ss) + xmul(Ma[1], s.p);
+        fl[3] = xmul(q3, ss) + xmul(Ma[2], s.p);
+        fl[4] = xmul(q4 + s.p, ss) -
+                xmul(s.p, xmul(ph.umf[0], Ma[0]) + xmul(ph.umf[1], Ma[1]) + xmul(ph.umf[2], Ma[2]));
+    }
     if (VISC) {
         // physical gradients without the J factor: dc/dx_k = sum_b M[b][k] G[b][c]
         double dx[4][3];
@@ -275,7 +290,8 @@ __device__ __forceinline__ void flux_values(double q0, double q1, double q2, dou
         for (int c = 0; c < 4; ++c)
 #pragma unroll
             for (int k = 0; k < 3; ++k)
-                dx[c][k] = xmul(pm.M[0][k], gr[c]) + xmul(pm.M[1][k], gr[4 + c]) + xmul(pm.M[2][k], gr[8 + c]);
+                dx[c][k] = DIAG ? xmul(pm.M[k][k], gr[4 * k + c])
+                                : xmul(pm.M[0][k], gr[c]) + xmul(pm.M[1][k], gr[4 + c]) + xmul(pm.M[2][k], gr[8 + c]);
         const double muj = xmul(ph.mu, pm.J);
         const double kap = xmul(kGamm1Prndtli, muj);
         const double div = xmul(2.0 / 3.0, dx[0][0] + dx[1][1] + dx[2][2]);
@@ -285,13 +301,25 @@ __device__ __forceinline__ void flux_values(double q0, double q1, double q2, dou
         const double txy = xmul(muj, dx[1][0] + dx[0][1]);
         const double tyz = xmul(muj, dx[2][1] + dx[1][2]);
         const double tzx = xmul(muj, dx[0][2] + dx[2][0]);
-        const double hx = xmul(kap, dx[3][0]) + xmul(s.u, txx) + xmul(s.v, txy) + xmul(s.w, tzx);
-        const double hy = xmul(kap, dx[3][1]) + xmul(s.u, txy) + xmul(s.v, tyy) + xmul(s.w, tyz);
-        const double hz = xmul(kap, dx[3][2]) + xmul(s.u, tzx) + xmul(s.v, tyz) + xmul(s.w, tzz);
-        fl[1] -= xmul(Ma[0], txx) + xmul(Ma[1], txy) + xmul(Ma[2], tzx);
-        fl[2] -= xmul(Ma[0], txy) + xmul(Ma[1], tyy) + xmul(Ma[2], tyz);
-        fl[3] -= xmul(Ma[0], tzx) + xmul(Ma[1], tyz) + xmul(Ma[2], tzz);
-        fl[4] -= xmul(Ma[0], hx) + xmul(Ma[1], hy) + xmul(Ma[2], hz);
+        // rows of the stress tensor: t[k] = (tau_kx, tau_ky, tau_kz)
+        const double t[3][3] = {{txx, txy, tzx}, {txy, tyy, tyz}, {tzx, tyz, tzz}};
+        if (DIAG) {
+            // only the AXIS column of tau and the AXIS component of h are needed
+            const double hA = xmul(kap, dx[3][AXIS]) + xmul(s.u, t[0][AXIS]) + xmul(s.v, t[1][AXIS]) +
+                              xmul(s.w, t[2][AXIS]);
+            fl[1] -= xmul(Ma[AXIS], t[0][AXIS]);
+            fl[2] -= xmul(Ma[AXIS], t[1][AXIS]);
+            fl[3] -= xmul(Ma[AXIS], t[2][AXIS]);
+            fl[4] -= xmul(Ma[AXIS], hA);
+        } else {
+            const double hx = xmul(kap, dx[3][0]) + xmul(s.u, txx) + xmul(s.v, txy) + xmul(s.w, tzx);
+            const double hy = xmul(kap, dx[3][1]) + xmul(s.u, txy) + xmul(s.v, tyy) + xmul(s.w, tyz);
+            const double hz = xmul(kap, dx[3][2]) + xmul(s.u, tzx) + xmul(s.v, tyz) + xmul(s.w, tzz);
+            fl[1] -= xmul(Ma[0], txx) + xmul(Ma[1], txy) + xmul(Ma[2], tzx);
+            fl[2] -= xmul(Ma[0], txy) + xmul(Ma[1], tyy) + xmul(Ma[2], tyz);
+            fl[3] -= xmul(Ma[0], tzx) + xmul(Ma[1], tyz) + xmul(Ma[2], tzz);
+            fl[4] -= xmul(Ma[0], hx) + xmul(Ma[1], hy) + xmul(Ma[2], hz);
+        }
     }
 }
 
@@ -310,7 +338,8 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
         for (int k = 0; k < 12; ++k) gr[k] = CG ? __ldcg(g + k * lmx + gi) : __ldg(g + k * lmx + gi);
     }
     const PointMet pm = point_met<FM>(ph, fm, lmx, gi);
-    flux_values<AXIS, VISC>(q0, q1, q2, q3, q4, gr, pm, ph, fl);
+    // the uniform grid of Phys is Cartesian: its metric matrix is diagonal
+    flux_values<AXIS, VISC, !FM>(q0, q1, q2, q3, q4, gr, pm, ph, fl);
 }
 
 // One tile of the flux pass (TL * 32 threads; sm holds 5 * TL line slots).

@@ -243,22 +243,26 @@ __device__ __forceinline__ void point_flux_mx(const float *__restrict__ sh, cons
         for (int k = 0; k < 12; ++k) gr[k] = (double)__ldg(g + k * lmx + gi);
     }
     const double rho = kRho0 + dr;
-    const double *Ma = ph.M[AXIS];
-    const double ss = Ma[0] * (u + ph.umf[0]) + Ma[1] * (v + ph.umf[1]) + Ma[2] * (wv + ph.umf[2]);
+    // the mixed form runs on the uniform Cartesian grid: the metric matrix is
+    // diagonal, so only the AXIS entries of the sums below are nonzero
+    const double mA = ph.M[AXIS][AXIS];
+    const double vel[3] = {u, v, wv};
+    const double ss = mA * (vel[AXIS] + ph.umf[AXIS]);
     // rho*H = gamma/(gamma-1) p + rho |u|^2 / 2 with p = p0 + dp
     const double rH = kGam * kHamm1 * (kP0 + dp) + 0.5 * rho * (u * u + v * v + wv * wv);
     double fl[5];
     fl[0] = rho * ss;
-    fl[1] = rho * u * ss + Ma[0] * dp;
-    fl[2] = rho * v * ss + Ma[1] * dp;
-    fl[3] = rho * wv * ss + Ma[2] * dp;
-    fl[4] = rH * ss - dp * (ph.umf[0] * Ma[0] + ph.umf[1] * Ma[1] + ph.umf[2] * Ma[2]);
+    fl[1] = rho * u * ss;
+    fl[2] = rho * v * ss;
+    fl[3] = rho * wv * ss;
+    fl[1 + AXIS] += mA * dp;
+    fl[4] = rH * ss - dp * (ph.umf[AXIS] * mA);
     if (VISC) {
         double dx[4][3];
 #pragma unroll
         for (int c = 0; c < 4; ++c)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) dx[c][k] = ph.M[0][k] * gr[c] + ph.M[1][k] * gr[4 + c] + ph.M[2][k] * gr[8 + c];
+            for (int k = 0; k < 3; ++k) dx[c][k] = ph.M[k][k] * gr[4 * k + c];
         const double muj = ph.mu * ph.J;
         const double kap = kGamm1Prndtli * muj;
         const double div = 2.0 / 3.0 * (dx[0][0] + dx[1][1] + dx[2][2]);
@@ -266,13 +270,13 @@ __device__ __forceinline__ void point_flux_mx(const float *__restrict__ sh, cons
         const double tzz = muj * (2.0 * dx[2][2] - div);
         const double txy = muj * (dx[1][0] + dx[0][1]), tyz = muj * (dx[2][1] + dx[1][2]);
         const double tzx = muj * (dx[0][2] + dx[2][0]);
-        const double hx = kap * dx[3][0] + u * txx + v * txy + wv * tzx;
-        const double hy = kap * dx[3][1] + u * txy + v * tyy + wv * tyz;
-        const double hz = kap * dx[3][2] + u * tzx + v * tyz + wv * tzz;
-        fl[1] -= Ma[0] * txx + Ma[1] * txy + Ma[2] * tzx;
-        fl[2] -= Ma[0] * txy + Ma[1] * tyy + Ma[2] * tyz;
-        fl[3] -= Ma[0] * tzx + Ma[1] * tyz + Ma[2] * tzz;
-        fl[4] -= Ma[0] * hx + Ma[1] * hy + Ma[2] * hz;
+        // rows of the stress tensor: t[k] = (tau_kx, tau_ky, tau_kz); only column AXIS is needed
+        const double t[3][3] = {{txx, txy, tzx}, {txy, tyy, tyz}, {tzx, tyz, tzz}};
+        const double hA = kap * dx[3][AXIS] + u * t[0][AXIS] + v * t[1][AXIS] + wv * t[2][AXIS];
+        fl[1] -= mA * t[0][AXIS];
+        fl[2] -= mA * t[1][AXIS];
+        fl[3] -= mA * t[2][AXIS];
+        fl[4] -= mA * hA;
     }
 #pragma unroll
     for (int m = 0; m < 5; ++m) flo[m] = (float)fl[m];
