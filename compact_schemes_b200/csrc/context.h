@@ -30,6 +30,11 @@ struct DeviceTables {
     DevTables<double> t64{};
     DevTables<float> t32{};
     int lt = 0;
+    // every lane's chunk shares lane 0's per-row factors (full chunks, the
+    // constant interior rows only: ChunkFactors); cfu holds them in FP32 as
+    // [f1, f2, b1, b2, -rca, -rcc][lt]
+    bool uniform = false;
+    float cfu[6 * 32] = {};
 };
 
 // key: n, scheme, nstart, nend, alpha_f bits

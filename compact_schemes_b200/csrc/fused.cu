@@ -287,6 +287,7 @@ static MixedArgs mixed_args(cs_solver *s, int a, int kind) {
     // CS_REFINE_FLUX: the gradient passes skip the refinement sweep (their
     // FP32 solve error only reaches the state through the viscous terms)
     m.refine = s->cfg.refine == CS_REFINE_FLUX ? (kind == 1) : s->cfg.refine;
+    m.fp32 = s->cfg.precision == CS_PREC_MIXED_F32;
     return m;
 }
 
@@ -459,7 +460,7 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         }
         s->active[a] = 1;
     }
-    if (cfg->precision != CS_PREC_FP64 && cfg->precision != CS_PREC_MIXED) {
+    if (cfg->precision != CS_PREC_FP64 && cfg->precision != CS_PREC_MIXED && cfg->precision != CS_PREC_MIXED_F32) {
         delete s;
         return set_error(CS_ERR_INVALID, "precision %d", cfg->precision);
     }
@@ -476,7 +477,7 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
             delete s;
             return set_error(CS_ERR_INVALID, "alpha_f %g: the filter needs -0.5 < alpha_f <= 0.5", cfg->alpha_f);
         }
-        if (cfg->filter == CS_FILTER_STAGE && cfg->precision == CS_PREC_MIXED) {
+        if (cfg->filter == CS_FILTER_STAGE && cfg->precision != CS_PREC_FP64) {
             delete s;
             return set_error(CS_ERR_UNSUPPORTED, "the mixed form filters after every step only");
         }
@@ -498,7 +499,7 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
         smem_max = 227 * 1024;
-    const size_t elem = cfg->precision == CS_PREC_MIXED ? sizeof(float) : sizeof(double);
+    const size_t elem = cfg->precision != CS_PREC_FP64 ? sizeof(float) : sizeof(double);
     for (int k = 0; k < 2; ++k)
         for (int a = 0; a < 3; ++a) {
             const int t = cfg->tile[k][a];
@@ -508,7 +509,7 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
             }
             if (t) s->tile[k][a] = t;
             // the mixed form compiles 16-line tiles for the z axis only
-            if (cfg->precision == CS_PREC_MIXED && a == 1) s->tile[k][a] = 8;
+            if (cfg->precision != CS_PREC_FP64 && a == 1) s->tile[k][a] = 8;
             if (!s->active[a]) continue;
             // a tile holds 4 (gradient) or 5 (flux) staged fields of full lines
             const size_t slot = (size_t)32 * s->tab[a]->lt + 1;
@@ -562,7 +563,7 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
         return set_error(CS_ERR_ALLOC, "solver scratch allocation failed");
     }
     cudaMemset(s->grad, 0, 12 * lmx * sizeof(double));
-    if (cfg->precision == CS_PREC_MIXED) {
+    if (cfg->precision != CS_PREC_FP64) {
         s->mixed = true;
         const bool okm = cudaMalloc(&s->sh32, 5 * lmx * sizeof(float)) == cudaSuccess &&
                          cudaMalloc(&s->grad32, 12 * lmx * sizeof(float)) == cudaSuccess &&

@@ -127,13 +127,62 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
 #ifndef CSB_MX_SOLVE_GROUP
 #define CSB_MX_SOLVE_GROUP 2
 #endif
+#ifndef CSB_CF_SOLVE_GROUP
+#define CSB_CF_SOLVE_GROUP 2
+#endif
+
+// FP32 solve of G lines with ChunkFactors (interface closure on both ends,
+// full chunks): interior right-hand sides in FP32, the four closure rows of
+// each line in FP64 (group_closure_rows), per-row factors from the kernel
+// parameters.  The results overwrite the lines.
+template <int LT, int G>
+__device__ __forceinline__ void solve_lines_cf(float *const (&lines)[G], int nf, int lane,
+                                               const DevTables<float> &tab, const ChunkFactors<LT> &U,
+                                               const Coeffs &cf) {
+    const int p = tab.p;
+    const double rows = group_closure_rows<LT, double, float, G>(lines, nf, tab.n, lane, cf);
+    float x[G][LT];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        double own2[2];
+        take_closure_rows(rows, g, lane, own2);
+        if (g < nf) deriv_rhs_cf<LT>(lines[g], p, lane, own2, x[g]);
+        else {
+#pragma unroll
+            for (int t = 0; t < LT; ++t) x[g][t] = 0.0f;
+        }
+    }
+    warp_solve_cf<LT, G>(U, tab, x, lane);
+    __syncwarp();
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        if (g >= nf) continue;
+        if (lane < p) {
+#pragma unroll
+            for (int t = 0; t < LT; ++t) lines[g][LineLayout<LT>::pos_ct(lane, t)] = x[g][t];
+        }
+    }
+}
 
 // The NF fields of this warp's line of the tile, CSB_MX_SOLVE_GROUP at a time
 // (one at a time for lines of more than 256 points when the refinement sweep
 // is compiled in: registers).
-template <int LT, int TL, int NF, bool REF>
+// CF: the lines have ChunkFactors (solve_lines_cf; no refinement sweep).
+template <int LT, int TL, int NF, bool REF, bool CF = false>
 __device__ __forceinline__ void solve_fields_mx(float *sm, int w, int lane, const DevTables<float> &tab,
-                                                int nstart, int nend, const Coeffs &cf) {
+                                                int nstart, int nend, const Coeffs &cf,
+                                                const ChunkFactors<LT> &U) {
+    if (CF) {
+        constexpr int G = CSB_CF_SOLVE_GROUP;
+#pragma unroll 1
+        for (int c = 0; c < NF; c += G) {
+            float *lines[G];
+#pragma unroll
+            for (int g = 0; g < G; ++g) lines[g] = field_line32<LT, TL>(sm, c + g < NF ? c + g : c, w);
+            solve_lines_cf<LT, G>(lines, NF - c, lane, tab, U, cf);
+        }
+        return;
+    }
     constexpr int G = (LT >= 16 && REF) ? 1 : CSB_MX_SOLVE_GROUP;
 #pragma unroll 1
     for (int c = 0; c < NF; c += G) {
@@ -162,11 +211,11 @@ __device__ __forceinline__ double pres_dev(double dr, double dT) { return (dr + 
 // ----------------------------------------------------------------------------
 // gradient pass (FIRST: reads the FP64 state, writes the shadow, reduces CFL)
 // ----------------------------------------------------------------------------
-template <int LT, int AXIS, int TL, bool FIRST, bool REF>
+template <int LT, int AXIS, int TL, bool FIRST, bool REF, bool CF = false>
 __global__ void __launch_bounds__(TL * 32, TL == 8 ? 2 : 1)
 k_grad_mx(const double *__restrict__ q, float *__restrict__ sh, float *__restrict__ g,
           DevTables<float> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend, Coeffs cf,
-          Phys ph, unsigned long long *__restrict__ dtacc) {
+          Phys ph, unsigned long long *__restrict__ dtacc, ChunkFactors<LT> U) {
     using L = LineLayout<LT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *sm = reinterpret_cast<float *>(smem_raw);
@@ -209,7 +258,7 @@ k_grad_mx(const double *__restrict__ q, float *__restrict__ sh, float *__restric
         field_line32<LT, TL>(sm, 3, l)[pj] = tp;
     });
     tile_sync<AXIS, TL>();
-    if (line0 + w < F) solve_fields_mx<LT, TL, 4, REF>(sm, w, lane, tab, nstart, nend, cf);
+    if (line0 + w < F) solve_fields_mx<LT, TL, 4, REF, CF>(sm, w, lane, tab, nstart, nend, cf, U);
     tile_sync<AXIS, TL>();
     tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         const int pj = L::pos(j);
@@ -282,21 +331,96 @@ __device__ __forceinline__ void point_flux_mx(const float *__restrict__ sh, cons
     for (int m = 0; m < 5; ++m) flo[m] = (float)fl[m];
 }
 
-template <int LT, int AXIS, int TL, int MODE, bool VISC, bool SHADOW_OUT, bool REF>
+// Uniform-grid constants of the flux in FP32.
+struct PhysF {
+    float mA[3];   // diagonal metric entries M[k][k]
+    float umf[3];  // moving-frame velocity
+    float muj;     // mu J
+    float kap;     // heat conduction coefficient mu J / ((gamma - 1) Pr)
+};
+__device__ __forceinline__ PhysF phys_f32(const Phys &ph) {
+    PhysF f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        f.mA[k] = (float)ph.M[k][k];
+        f.umf[k] = (float)ph.umf[k];
+    }
+    f.muj = (float)(ph.mu * ph.J);
+    f.kap = (float)(kGamm1Prndtli * ph.mu * ph.J);
+    return f;
+}
+
+// point_flux_mx evaluated in FP32 (the flux arithmetic of the mixed form on
+// lines with ChunkFactors), divided by the pass's metric entry
+// mA = M[AXIS][AXIS]: every term of F[m][AXIS] on the uniform grid carries
+// exactly one factor mA and the compact derivative is linear, so the pass
+// multiplies the derivative by mA instead.  Leaving the factor out, and
+// forming each value with fused multiply-adds around its largest term, keeps
+// the FP32 rounding of the flux values (which the derivative amplifies by
+// about 1 / h) near one rounding per value, as when they are evaluated in
+// FP64 and rounded once.  The pressure enters as its deviation
+// p - p0 = (drho + dT + drho dT) / gamma.
+template <int AXIS, bool VISC>
+__device__ __forceinline__ void point_flux_f32(const float *__restrict__ sh, const float *__restrict__ g,
+                                               int64_t lmx, int64_t gi, const PhysF &pf, float (&fl)[5]) {
+    const float dr = __ldg(sh + gi), u = __ldg(sh + lmx + gi), v = __ldg(sh + 2 * lmx + gi);
+    const float wv = __ldg(sh + 3 * lmx + gi), dT = __ldg(sh + 4 * lmx + gi);
+    float gr[12];
+    if (VISC) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gr[k] = __ldg(g + k * lmx + gi);
+    }
+    constexpr float gami = (float)(1.0 / kGam), hamm1 = (float)kHamm1, cp0 = (float)(kGam * kHamm1 * kP0);
+    const float dpg = fmaf(dr, dT, dr + dT);  // gamma (p - p0)
+    const float dp = dpg * gami;
+    const float vel[3] = {u, v, wv};
+    const float sp = vel[AXIS] + pf.umf[AXIS];  // contravariant velocity / mA
+    const float rsp = fmaf(dr, sp, sp);         // rho * sp
+    fl[0] = rsp;
+    fl[1] = rsp * u;
+    fl[2] = rsp * v;
+    fl[3] = rsp * wv;
+    fl[1 + AXIS] = fmaf(rsp, vel[AXIS], dp);
+    // rho H = gamma p / (gamma - 1) + rho |u|^2 / 2 = cp0 + dpg / (gamma - 1) + rho |u|^2 / 2
+    const float q2 = fmaf(u, u, fmaf(v, v, wv * wv));
+    const float rest = fmaf(0.5f * (1.0f + dr), q2, hamm1 * dpg);
+    fl[4] = fmaf(cp0, sp, rest * sp) - dp * pf.umf[AXIS];
+    if (VISC) {
+        float dx[4][3];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) dx[c][k] = pf.mA[k] * gr[4 * k + c];
+        const float div = (2.0f / 3.0f) * (dx[0][0] + dx[1][1] + dx[2][2]);
+        float t[3];  // column AXIS of the stress tensor
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            t[k] = k == AXIS ? pf.muj * (2.0f * dx[k][k] - div) : pf.muj * (dx[k][AXIS] + dx[AXIS][k]);
+        const float hA = fmaf(pf.kap, dx[3][AXIS], fmaf(u, t[0], fmaf(v, t[1], wv * t[2])));
+        fl[1] -= t[0];
+        fl[2] -= t[1];
+        fl[3] -= t[2];
+        fl[4] -= hA;
+    }
+}
+
+template <int LT, int AXIS, int TL, int MODE, bool VISC, bool SHADOW_OUT, bool REF, bool CF = false>
 __global__ void __launch_bounds__(TL * 32, TL == 8 ? 2 : 1)
 k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__restrict__ rhs,
           const double *__restrict__ qn, double *__restrict__ qout, float *__restrict__ sh_out,
           double *__restrict__ drva, DevTables<float> tab, int lxi, int let, int64_t lmx, int64_t F,
-          int nstart, int nend, Coeffs cf, Phys ph, RkParams rk) {
+          int nstart, int nend, Coeffs cf, Phys ph, RkParams rk, ChunkFactors<LT> U) {
     using L = LineLayout<LT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *sm = reinterpret_cast<float *>(smem_raw);
     const int n = tab.n;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t line0 = (int64_t)blockIdx.x * TL;
+    const PhysF pf = phys_f32(ph);
     tile_for_each<AXIS, TL, CSB_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         float fl[5];
-        point_flux_mx<AXIS, VISC>(sh, g, lmx, gi, ph, fl);
+        if (CF) point_flux_f32<AXIS, VISC>(sh, g, lmx, gi, pf, fl);
+        else point_flux_mx<AXIS, VISC>(sh, g, lmx, gi, ph, fl);
         const int pj = L::pos(j);
 #pragma unroll
         for (int m = 0; m < 5; ++m) field_line32<LT, TL>(sm, m, l)[pj] = fl[m];
@@ -304,13 +428,13 @@ k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__re
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
     if (fidx < F) {
-        solve_fields_mx<LT, TL, 5, REF>(sm, w, lane, tab, nstart, nend, cf);
+        solve_fields_mx<LT, TL, 5, REF, CF>(sm, w, lane, tab, nstart, nend, cf, U);
         if (drva) {
             __syncwarp();
             if (lane < 10) {
                 const int m = lane % 5, face = lane / 5;
-                drva[(int64_t)(face * 5 + m) * F + fidx] =
-                    (double)field_line32<LT, TL>(sm, m, w)[L::pos(face ? n - 1 : 0)];
+                const double dv = (double)field_line32<LT, TL>(sm, m, w)[L::pos(face ? n - 1 : 0)];
+                drva[(int64_t)(face * 5 + m) * F + fidx] = CF ? ph.M[AXIS][AXIS] * dv : dv;
             }
         }
     }
@@ -321,11 +445,17 @@ k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__re
         dtk = xmul(dt / rk.div, ph.J);
         if (rk.dt_out && blockIdx.x == 0 && threadIdx.x == 0) *rk.dt_out = dt;
     }
+    // CF kernels solved F / mA (point_flux_f32): the derivative is scaled here
+    const float mA32 = pf.mA[AXIS];
+    const double mA64 = ph.M[AXIS][AXIS];
     if (MODE == kWrite) {
         tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
             const int pj = L::pos(j);
 #pragma unroll
-            for (int m = 0; m < 5; ++m) rhs[m * lmx + gi] = field_line32<LT, TL>(sm, m, l)[pj];
+            for (int m = 0; m < 5; ++m) {
+                const float dv = field_line32<LT, TL>(sm, m, l)[pj];
+                rhs[m * lmx + gi] = CF ? mA32 * dv : dv;
+            }
         });
     } else {
         constexpr int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK);
@@ -344,12 +474,16 @@ k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__re
                 const int pj = L::pos(j);
                 if (MODE == kAccum) {
 #pragma unroll
-                    for (int m = 0; m < 5; ++m) rhs[m * lmx + gi] = rv[p][m] + field_line32<LT, TL>(sm, m, l)[pj];
+                    for (int m = 0; m < 5; ++m) {
+                        const float dv = field_line32<LT, TL>(sm, m, l)[pj];
+                        rhs[m * lmx + gi] = CF ? fmaf(mA32, dv, rv[p][m]) : rv[p][m] + dv;
+                    }
                 } else {
                     double qo[5];
 #pragma unroll
                     for (int m = 0; m < 5; ++m) {
-                        const double r = (double)rv[p][m] + (double)field_line32<LT, TL>(sm, m, l)[pj];
+                        const double dv = (double)field_line32<LT, TL>(sm, m, l)[pj];
+                        const double r = CF ? fma(mA64, dv, (double)rv[p][m]) : (double)rv[p][m] + dv;
                         qo[m] = qv[p][m] - xmul(dtk, r);
                         qout[m * lmx + gi] = qo[m];
                     }
@@ -371,18 +505,43 @@ struct MixedArgs {
     float *grad;    // [3][4][lmx]
     float *rhs;     // [5][lmx]
     int refine;
+    int fp32;       // FP32 interior arithmetic where the line has ChunkFactors
 };
+
+// The pass runs the ChunkFactors kernels: FP32 interior arithmetic asked for,
+// no refinement sweep, and the line's tables uniform.
+inline bool use_cf(const MixedArgs &a) { return a.fp32 && !a.refine && a.base.tab->uniform; }
+
+template <int LT>
+ChunkFactors<LT> chunk_factors_of(const DeviceTables &dt) {
+    ChunkFactors<LT> U{};
+    if (!dt.uniform || dt.lt != LT) return U;
+    for (int t = 0; t < LT; ++t) {
+        U.f1[t] = dt.cfu[t];
+        U.f2[t] = dt.cfu[LT + t];
+        U.b1[t] = dt.cfu[2 * LT + t];
+        U.b2[t] = dt.cfu[3 * LT + t];
+        U.nra[t] = dt.cfu[4 * LT + t];
+        U.nrc[t] = dt.cfu[5 * LT + t];
+    }
+    return U;
+}
 
 template <int LT, int AXIS, int TL>
 int launch_grad_mx_t(const MixedArgs &a, const double *q, bool first, cudaStream_t st) {
     const size_t smem = (size_t)4 * TL * LineLayout<LT>::kSlot * sizeof(float);
-    auto kern = first ? (a.refine ? k_grad_mx<LT, AXIS, TL, true, true> : k_grad_mx<LT, AXIS, TL, true, false>)
-                      : (a.refine ? k_grad_mx<LT, AXIS, TL, false, true> : k_grad_mx<LT, AXIS, TL, false, false>);
+    const bool cfp = use_cf(a);
+    auto kern = first ? (a.refine ? k_grad_mx<LT, AXIS, TL, true, true>
+                                  : (cfp ? k_grad_mx<LT, AXIS, TL, true, false, true> : k_grad_mx<LT, AXIS, TL, true, false>))
+                      : (a.refine ? k_grad_mx<LT, AXIS, TL, false, true>
+                                  : (cfp ? k_grad_mx<LT, AXIS, TL, false, false, true>
+                                         : k_grad_mx<LT, AXIS, TL, false, false>));
     if (int rc = set_smem(kern, smem)) return rc;
     const PassArgs &b = a.base;
     const unsigned blocks = (unsigned)((b.F + TL - 1) / TL);
     kern<<<blocks, TL * 32, smem, st>>>(q, a.shadow, a.grad + (int64_t)AXIS * 4 * b.lmx, b.tab->t32, b.lxi,
-                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, b.dtacc);
+                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, b.dtacc,
+                                        chunk_factors_of<LT>(*b.tab));
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }
@@ -394,18 +553,22 @@ int launch_flux_mx_t(const MixedArgs &a, const double *qn, double *qout, bool sh
     const PassArgs &b = a.base;
     // the shadow is written only by the RK modes
     constexpr bool kRk = MODE >= kAccumRk;
-    auto pick = [&](auto ref) {
+    auto pick = [&](auto ref, auto cfv) {
         constexpr bool R = decltype(ref)::value;
-        return b.viscous ? (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, true, kRk, R>
-                                              : k_flux_mx<LT, AXIS, TL, MODE, true, false, R>)
-                         : (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, false, kRk, R>
-                                              : k_flux_mx<LT, AXIS, TL, MODE, false, false, R>);
+        constexpr bool C = decltype(cfv)::value;
+        return b.viscous ? (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, true, kRk, R, C>
+                                              : k_flux_mx<LT, AXIS, TL, MODE, true, false, R, C>)
+                         : (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, false, kRk, R, C>
+                                              : k_flux_mx<LT, AXIS, TL, MODE, false, false, R, C>);
     };
-    auto kern = a.refine ? pick(std::true_type{}) : pick(std::false_type{});
+    auto kern = a.refine ? pick(std::true_type{}, std::false_type{})
+                         : (use_cf(a) ? pick(std::false_type{}, std::true_type{})
+                                      : pick(std::false_type{}, std::false_type{}));
     if (int rc = set_smem(kern, smem)) return rc;
     const unsigned blocks = (unsigned)((b.F + TL - 1) / TL);
     kern<<<blocks, TL * 32, smem, st>>>(a.shadow, a.grad, a.rhs, qn, qout, a.shadow, drva, b.tab->t32, b.lxi,
-                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, rk);
+                                        b.let, b.lmx, b.F, b.nstart, b.nend, b.cf, b.ph, rk,
+                                        chunk_factors_of<LT>(*b.tab));
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }

@@ -136,6 +136,117 @@ __device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][L
     }
 }
 
+// Per-row factors of a line whose lanes all share them: every chunk is full
+// (n a multiple of LT) and the matrix rows that shape a chunk's elimination
+// are the constant interior rows, as for the compact derivative with the
+// interface (single-rank periodic) closure on both ends.  Only the reduced
+// system then differs between lanes.  The factors travel by value in the
+// kernel's parameters, so the solve reads them as constants instead of
+// loading six per-lane table entries per row.  nra / nrc are the negated
+// spike coefficients (rca / rcc of the tables).
+template <int LT>
+struct ChunkFactors {
+    float f1[LT], f2[LT], b1[LT], b2[LT], nra[LT], nrc[LT];
+};
+
+// warp_solve for lines with ChunkFactors (all chunks full, no cyclic
+// correction): FP32, NV right-hand sides held as d[v][t].  The structure of
+// the tables fixes fwd2 = 0 for rows 0 and 1 of a chunk, bwd1 = 1 and bwd2 = 0
+// for row LT - 2, and bwd1 = 1 for rows 1 .. LT - 3; those products are
+// left out.  All 32 lanes must call it.
+template <int LT, int NV>
+__device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT> &U, const DevTables<float> &T,
+                                              float (&d)[NV][LT], int lane) {
+    static_assert(LT >= 2, "chunk");
+#pragma unroll
+    for (int t = 0; t < LT; ++t)
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            d[v][t] = t < 2 ? U.f1[t] * d[v][t] : fmaf(U.f2[t], d[v][t - 1], U.f1[t] * d[v][t]);
+#pragma unroll
+    for (int t = LT - 3; t >= 0; --t)
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            d[v][t] = t == 0 ? fmaf(U.b2[0], d[v][1], U.b1[0] * d[v][0]) : fmaf(U.b2[t], d[v][t + 1], d[v][t]);
+    float y0[NV], y1[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        y0[v] = d[v][0];
+        y1[v] = d[v][LT - 1];
+    }
+    {
+        const float ka = T.k1[lane], kb = T.k2[lane], kc = T.k1[32 + lane], kd = T.k2[32 + lane];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const float up1 = __shfl_up_sync(0xffffffffu, y1[v], 1);
+            const float dn0 = __shfl_down_sync(0xffffffffu, y0[v], 1);
+            const float n0 = y0[v] - ka * up1 - kb * y1[v];
+            const float n1 = y1[v] - kc * y0[v] - kd * dn0;
+            y0[v] = n0;
+            y1[v] = n1;
+        }
+    }
+#pragma unroll
+    for (int s = 1; s < kPcrSteps; ++s) {
+        if (s >= T.pcr) break;
+        const int dl = 1 << (s - 1);
+        const float ka = T.k1[s * 64 + lane], kb = T.k2[s * 64 + lane];
+        const float kc = T.k1[s * 64 + 32 + lane], kd = T.k2[s * 64 + 32 + lane];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const float u0 = __shfl_up_sync(0xffffffffu, y0[v], dl);
+            const float d0 = __shfl_down_sync(0xffffffffu, y0[v], dl);
+            const float u1 = __shfl_up_sync(0xffffffffu, y1[v], dl);
+            const float d1 = __shfl_down_sync(0xffffffffu, y1[v], dl);
+            y0[v] = y0[v] - ka * u0 - kb * d0;
+            y1[v] = y1[v] - kc * u1 - kd * d1;
+        }
+    }
+    const float ib0 = T.invb[lane], ib1 = T.invb[32 + lane];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const float X0 = y0[v] * ib0, X1 = y1[v] * ib1;
+        d[v][0] = X0;
+#pragma unroll
+        for (int t = 1; t + 1 < LT; ++t) d[v][t] = fmaf(U.nrc[t], X1, fmaf(U.nra[t], X0, d[v][t]));
+        d[v][LT - 1] = X1;
+    }
+}
+
+// Right-hand side of the compact derivative in FP32 for a line with
+// ChunkFactors (p = n / LT full chunks, interface closure on both ends):
+// interior rows aa (f[j+1] - f[j-1]) + bb (f[j+2] - f[j-2]), differences
+// first; rows 0, 1 (lane 0) and n-1, n-2 (lane p-1) are the closure rows
+// `own2` formed in FP64 by group_closure_rows / take_closure_rows.  Lanes
+// >= p hold no rows.  `f` is the line in LineLayout<LT> order.
+template <int LT>
+__device__ __forceinline__ void deriv_rhs_cf(const float *f, int p, int lane, const double (&own2)[2],
+                                             float (&d)[LT]) {
+    using L = LineLayout<LT>;
+    float w[LT + 4];
+#pragma unroll
+    for (int k = 0; k < LT + 4; ++k) {
+        const int t = (k + LT - 2) % LT;
+        const int dc = k < 2 ? -1 : (k >= LT + 2 ? 1 : 0);
+        w[k] = f[L::pos_ct(lane + dc, t)];
+    }
+    constexpr float aa = (float)kAa, bb = (float)kBb;
+#pragma unroll
+    for (int t = 0; t < LT; ++t) d[t] = fmaf(bb, w[t + 4] - w[t], aa * (w[t + 3] - w[t + 1]));
+    if (lane == 0) {
+        d[0] = (float)own2[0];
+        d[1] = (float)own2[1];
+    }
+    if (lane == p - 1) {
+        d[LT - 1] = (float)(-own2[0]);
+        d[LT - 2] = (float)(-own2[1]);
+    }
+    if (lane >= p) {
+#pragma unroll
+        for (int t = 0; t < LT; ++t) d[t] = 0.0f;
+    }
+}
+
 // Select d[t] for a runtime t without dynamic register indexing.
 template <int LT, typename CT>
 __device__ __forceinline__ void set_at(CT (&d)[LT], int t, CT val) {

@@ -72,6 +72,27 @@ static std::vector<double> pack(const HostTables &h, bool fp32 = false) {
     return v;
 }
 
+// Whether all lanes of a table set share lane 0's per-row chunk factors
+// (every chunk full, no cyclic correction), and those factors in FP32.  The
+// comparison is exact, so a line qualifies only when its tables say so.
+static void chunk_factors(const HostTables &h, bool &uniform, float *cfu) {
+    uniform = !h.cyclic && h.lt <= 32 && h.n == h.p * h.lt && h.p >= 2;
+    const std::vector<double> *tabs[6] = {&h.fwd1, &h.fwd2, &h.bwd1, &h.bwd2, &h.rca, &h.rcc};
+    for (int k = 0; k < 6 && uniform; ++k)
+        for (int t = 0; t < h.lt && uniform; ++t)
+            for (int lane = 1; lane < h.p; ++lane)
+                if ((*tabs[k])[(size_t)t * 32 + lane] != (*tabs[k])[(size_t)t * 32]) {
+                    uniform = false;
+                    break;
+                }
+    if (!uniform) return;
+    for (int k = 0; k < 6; ++k)
+        for (int t = 0; t < h.lt; ++t) {
+            const double v = (*tabs[k])[(size_t)t * 32];
+            cfu[k * h.lt + t] = (float)(k >= 4 ? -v : v);
+        }
+}
+
 static bool host_tables_for(int n, int scheme, int nstart, int nend, double af, HostTables &h) {
     std::vector<double> a(n), b(n), c(n);
     bool cyclic = false;
@@ -127,6 +148,7 @@ const DeviceTables *TableCache::get(int n, int scheme, int nstart, int nend, dou
     bind(dt->t64, dt->d64, dt->host);
     bind(dt->t32, dt->d32, dt->host);
     dt->lt = dt->host.lt;
+    chunk_factors(dt->host, dt->uniform, dt->cfu);
     map_[key] = dt;
     return dt;
 }

@@ -25,6 +25,7 @@ class SolverConfig(ctypes.Structure):
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_MIXED_F32 = 2  # mixed, FP32 interior arithmetic (fluxes, interior RHS) on uniform lines
 REFINE_NONE = 0  # mixed: no refinement sweep (the measured state error is the same)
 REFINE_ALL = 1   # mixed: a refinement sweep after every FP32 line solve
 REFINE_FLUX = 2  # mixed: refinement in the flux passes only

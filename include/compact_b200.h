@@ -260,6 +260,12 @@ typedef struct cs_solver cs_solver;
 #define CS_PREC_FP64 0  /* plain FP64 */
 #define CS_PREC_MIXED 1 /* FP32 fluxes and line solves (FP64 right-hand sides, refinement
                            as cfg.refine), FP64 state, RK accumulation and thermodynamics */
+#define CS_PREC_MIXED_F32 2 /* as CS_PREC_MIXED, with FP32 arithmetic in the interior: fluxes
+                               evaluated in FP32, interior right-hand sides in FP32 (closure
+                               rows in FP64) and per-row solver factors as constants, on every
+                               axis whose lines have uniform chunk factors (interface or periodic
+                               closure, length a multiple of the chunk) and no refinement sweep;
+                               other axes run as CS_PREC_MIXED */
 
 #define CS_REFINE_NONE 0 /* mixed: no refinement sweep */
 #define CS_REFINE_ALL 1  /* mixed: a refinement sweep after every FP32 line solve */

@@ -1,6 +1,8 @@
 """Mixed-precision form: FP32 fluxes and line solves (FP64 right-hand sides,
 an optional FP64-residual refinement sweep), FP64 state, RK accumulation and
-thermodynamics.
+thermodynamics.  Precision 2 (CS_PREC_MIXED_F32) also evaluates the fluxes
+and the interior right-hand sides in FP32 on axes whose lines have uniform
+chunk factors, keeping the closure rows in FP64.
 
 Target: relative state error <= 1e-6 per field after 100 RK steps
 against the FP64 path.  Relative error of a field f: max|f - f64| / max|f64|.
@@ -27,14 +29,15 @@ def make(dims, precision, **kw):
     return cs.Solver(cs.tgv_config(None, dims=dims, precision=precision, **kw))
 
 
-@pytest.mark.parametrize("refine", [1, 0, 2])
-def test_mixed_rhs_vs_oracle(cuda, refine):
-    """Mixed RHS against the FP64 oracle, relative to the size of the summed terms."""
+@pytest.mark.parametrize("prec,refine,dims", [(1, 1, (48, 40, 32)), (1, 0, (48, 40, 32)), (1, 2, (48, 40, 32)),
+                                               (2, 0, (48, 40, 32)), (2, 0, (50, 33, 36))])
+def test_mixed_rhs_vs_oracle(cuda, prec, refine, dims):
+    """Mixed RHS against the FP64 oracle, relative to the size of the summed terms
+    (33-point lines are not a multiple of their chunk: that axis runs as precision 1)."""
     import torch
-    dims = (48, 40, 32)
     q = O.tgv_init(dims, MACH, 1e-4, 0)
     ref, scale = O.rhs(q, MU, O.uniform_metrics(*dims), dims, [[1] * 3, [1] * 3], with_scale=True)
-    s = make(dims, 1, refine=refine)
+    s = make(dims, prec, refine=refine)
     out = torch.zeros(q.size, dtype=torch.float64, device="cuda")
     s.rhs(torch.from_numpy(q).cuda(), out)
     torch.cuda.synchronize()
@@ -43,8 +46,8 @@ def test_mixed_rhs_vs_oracle(cuda, refine):
     assert err < 2e-6, err
 
 
-@pytest.mark.parametrize("refine", [0, 1, 2])
-def test_mixed_100_steps_within_1e6(cuda, refine):
+@pytest.mark.parametrize("prec,refine", [(1, 0), (1, 1), (1, 2), (2, 0)])
+def test_mixed_100_steps_within_1e6(cuda, prec, refine):
     import torch
     import compact_schemes_b200 as cs
     dims = (64, 64, 64)
@@ -52,18 +55,19 @@ def test_mixed_100_steps_within_1e6(cuda, refine):
     q0 = torch.empty(5 * n, dtype=torch.float64, device="cuda")
     cs.tgv_init(q0, dims, MACH, 1e-4, 0)
     qp, qm = q0.clone(), q0.clone()
-    sp, sm = make(dims, 0), make(dims, 1, refine=refine)
+    sp, sm = make(dims, 0), make(dims, prec, refine=refine)
     for _ in range(100):
         sp.step(qp, 0.0)
         sm.step(qm, 0.0)
     torch.cuda.synchronize()
     errs = per_field(qm, qp, n)
-    print("mixed (refine %d) vs FP64 after 100 steps at 64^3, per field:" % refine, errs)
+    print("mixed %d (refine %d) vs FP64 after 100 steps at 64^3, per field:" % (prec, refine), errs)
     assert max(errs[:3] + errs[4:]) <= 1e-6, errs
     assert errs[3] <= 1e-5, errs
 
 
-def test_mixed_512_gcbc_100_steps(cuda):
+@pytest.mark.parametrize("prec", [1, 2])
+def test_mixed_512_gcbc_100_steps(cuda, prec):
     """512^3 mixed form with non-reflective GCBC on the x faces, periodic y/z,
     100 RK steps; per-field error against the FP64 path (itself checked against
     the CPU oracle at <= 256^3)."""
@@ -80,7 +84,7 @@ def test_mixed_512_gcbc_100_steps(cuda):
         sp.step(qp, 0.0)
     sp.close()
     qm = q0
-    sm = make(dims, 1, nbc=nbc, gcbc=True)
+    sm = make(dims, prec, nbc=nbc, gcbc=True)
     for _ in range(100):
         sm.step(qm, 0.0)
     torch.cuda.synchronize()
