@@ -294,6 +294,12 @@ static MixedArgs mixed_args(cs_solver *s, int a, int kind) {
 static int grad_pass_mx(cs_solver *s, int a, const double *q, bool first, cudaStream_t st) {
     PassTimer pt(s, st, kPassGradX + a);
     const MixedArgs m = mixed_args(s, a, 0);
+    // the TMA form reads the FP32 shadow, which the first pass of a step writes
+    if (s->tma[a] && !first) {
+        if (a == 0) return launch_grad_mx_tma<0>(m, s->d, s->err, st);
+        if (a == 1) return launch_grad_mx_tma<1>(m, s->d, s->err, st);
+        return launch_grad_mx_tma<2>(m, s->d, s->err, st);
+    }
     if (a == 0) return launch_grad_mx<0>(m, q, first, st);
     if (a == 1) return launch_grad_mx<1>(m, q, first, st);
     return launch_grad_mx<2>(m, q, first, st);
@@ -534,10 +540,12 @@ int cs_solver_create(cs_solver **out, const cs_solver_config *cfg) {
             s->can[k][a] = (bytes(8) <= (size_t)smem_max ? 1 : 0) |
                            (a > 0 && !(elem == 4 && a == 1) && bytes(16) <= (size_t)smem_max ? 2 : 0) |
                            (pl_fits ? 4 : 0);
-            if (k == 0 && cfg->precision == CS_PREC_FP64) {
+            if (k == 0) {
                 TmaGeom g;
                 size_t tb = 0;
-                if (tma_grad_geometry(a, s->d, s->tab[a]->lt, smem_max, g, tb)) s->can[0][a] |= 8;
+                if (cfg->precision == CS_PREC_FP64 ? tma_grad_geometry(a, s->d, s->tab[a]->lt, smem_max, g, tb)
+                                                   : tma_grad_mx_geometry(a, s->d, s->tab[a]->lt, smem_max, g, tb))
+                    s->can[0][a] |= 8;
                 s->tma[a] = cfg->schedule == CS_SCHED_TMA && (s->can[0][a] & 8);
             }
             if (!s->pl[k][a] && !(k == 0 && s->tma[a]) && bytes(s->tile[k][a]) > (size_t)smem_max) {

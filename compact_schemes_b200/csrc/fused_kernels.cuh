@@ -555,6 +555,9 @@ struct TmaGeom {
 // does not apply (lines longer than 512 points, row strides that are not
 // multiples of 16 bytes, or more shared memory than smem_max).
 bool tma_grad_geometry(int axis, const cs_dcomp &d, int lt, int smem_max, TmaGeom &g, size_t &smem_bytes);
+// The same for the mixed form's gradient passes: the four FP32 shadow fields
+// (u, v, w, T - T0) in tiles of 8 lines (4 for lines of 257-512 points).
+bool tma_grad_mx_geometry(int axis, const cs_dcomp &d, int lt, int smem_max, TmaGeom &g, size_t &smem_bytes);
 // TMA-staged gradient pass along AXIS (tma_grad_axis{0,1,2}.cu); err receives
 // a nonzero code if a staging copy did not complete in time.
 template <int AXIS>

@@ -616,6 +616,11 @@ int launch_flux_mx_pl(const MixedArgs &m, int mode, const double *qn, double *qo
                       double *drva, const RkParams &rk, cudaStream_t st);
 template <int AXIS>
 int launch_grad_mx(const MixedArgs &a, const double *q, bool first, cudaStream_t st);
+// TMA-staged gradient pass of the mixed form (not the first of a step: it
+// reads the FP32 shadow), tma_grad_mx_axis{0,1,2}.cu; err receives a nonzero
+// code if a staging copy did not complete in time.
+template <int AXIS>
+int launch_grad_mx_tma(const MixedArgs &m, const cs_dcomp &d, int *err, cudaStream_t st);
 template <int AXIS>
 int launch_flux_mx(const MixedArgs &a, int mode, const double *qn, double *qout, bool shadow_out,
                    double *drva, const RkParams &rk, cudaStream_t st);

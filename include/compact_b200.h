@@ -281,8 +281,10 @@ typedef struct cs_solver cs_solver;
 #define CS_FILTER_STAGE 2 /* the same after every RK stage (FP64 only) */
 
 #define CS_SCHED_TMA 3      /* gradient passes: persistent CTAs whose pencils of the state are
-                               staged into shared memory by TMA two tiles ahead (FP64, lines of
-                               up to 512 points, even row lengths; else one-phase); flux passes
+                               staged into shared memory by TMA two tiles ahead (FP64: lines of
+                               up to 512 points, even row lengths; mixed: the FP32 shadow of every
+                               gradient pass but a step's first, lines of up to 512 points, row
+                               lengths and points a multiple of 4; else one-phase); flux passes
                                one-phase */
 
 typedef struct {
