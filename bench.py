@@ -66,21 +66,44 @@ def parse():
     return p.parse_args()
 
 
+FIELDS = ["rho", "rho_u", "rho_v", "rho_w", "rho_E"]
+
+
+def state_errors(q, qref, lmx):
+    """Per-field error of a state against a reference state: relative to each
+    field's maximum, and for the momenta also relative to the largest momentum."""
+    errs, errs_m = {}, {}
+    mmax = max(float(qref[i * lmx:(i + 1) * lmx].abs().max()) for i in (1, 2, 3))
+    for i, name in enumerate(FIELDS):
+        a, b = q[i * lmx:(i + 1) * lmx], qref[i * lmx:(i + 1) * lmx]
+        d = float((a - b).abs().max())
+        errs[name] = d / float(b.abs().max())
+        if 1 <= i <= 3:
+            errs_m[name] = d / mmax
+    return errs, errs_m
+
+
 def mixed_512_gcbc_section(args, steps=6):
-    """Mixed form of the Taylor-Green box at 512^3 with non-reflective GCBC x
-    faces and periodic y/z: both forms autotuned, ms per step, and the
-    per-field error of the mixed state against the FP64 state after the same
-    steps from the same initial state."""
+    """Mixed forms of the Taylor-Green box at 512^3 with non-reflective GCBC x
+    faces and periodic y/z, all autotuned: ms per step, and the per-field error
+    of each mixed state against the FP64 state after the same steps from the
+    same initial state.  `mixed` is the FP32-interior form (CS_PREC_MIXED_F32:
+    its x lines have physical closures and run the table solve; y and z the
+    ChunkFactors solve); `mixed_fp64_rhs` forms every right-hand side and flux
+    in FP64 (CS_PREC_MIXED); `mixed_refinement_sweep_on` adds the FP64-residual
+    refinement sweep to the latter."""
     import torch
     import compact_schemes_b200 as cs
+    from compact_schemes_b200.solver import PREC_MIXED, PREC_MIXED_F32, REFINE_ALL
     n = 512
     lmx = n ** 3
     nbc = [[cs.BC_NON_REFLECTIVE, cs.BC_PERIODIC, cs.BC_PERIODIC]] * 2
-    from compact_schemes_b200.solver import REFINE_ALL
-    out, states = {}, {}
-    for prec in (0, 1, 2):  # plain, mixed, mixed with the refinement sweep
+    variants = [("plain", 0, 0), ("mixed", PREC_MIXED_F32, 0), ("mixed_fp64_rhs", PREC_MIXED, 0),
+                ("mixed_refinement_sweep_on", PREC_MIXED, REFINE_ALL)]
+    out, qref = {}, None
+    for key, prec, refine in variants:
         s = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, nbc=nbc, gcbc=True,
-                                    precision=min(prec, 1), refine=REFINE_ALL if prec == 2 else 0))
+                                    precision=prec, refine=refine))
         q = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
         cs.tgv_init(q, (n, n, n), MACH, 1e-4, 0)
         choice = s.autotune(q, reps=1)
@@ -92,36 +115,24 @@ def mixed_512_gcbc_section(args, steps=6):
             s.step(q)
         e1.record()
         torch.cuda.synchronize()
-        out[prec] = {"ms_per_step": e0.elapsed_time(e1) / steps,
-                     "schedule": {"%s_%s" % ("grad" if k == 0 else "flux", "xyz"[a]): v
-                                  for (k, a), v in choice.items()}}
-        if prec < 2:
-            states[prec] = q
+        ms = e0.elapsed_time(e1) / steps
+        out[key] = {"ms_per_step": ms, "value": lmx * 4 / (ms * 1e-3) / 1e6,
+                    "schedule": {"%s_%s" % ("grad" if k == 0 else "flux", "xyz"[a]): v
+                                 for (k, a), v in choice.items()}}
+        if qref is None:
+            qref = q
         else:
-            d2 = [float((q[i * lmx:(i + 1) * lmx] - states[0][i * lmx:(i + 1) * lmx]).abs().max() /
-                        states[0][i * lmx:(i + 1) * lmx].abs().max()) for i in range(5)]
-            out[prec]["rel_err_vs_fp64_per_field"] = dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_E"], d2))
+            out[key]["speedup_vs_plain"] = out["plain"]["ms_per_step"] / ms
+            out[key]["rel_err_vs_fp64_per_field"], out[key]["rel_err_momentum_vs_max_momentum"] = \
+                state_errors(q, qref, lmx)
             del q
         s.close()
-    errs, errs_m = {}, {}
-    mmax = max(float(states[0][i * lmx:(i + 1) * lmx].abs().max()) for i in (1, 2, 3))
-    for i, name in enumerate(["rho", "rho_u", "rho_v", "rho_w", "rho_E"]):
-        a, b = states[1][i * lmx:(i + 1) * lmx], states[0][i * lmx:(i + 1) * lmx]
-        d = float((a - b).abs().max())
-        errs[name] = d / float(b.abs().max())
-        if 1 <= i <= 3:
-            errs_m[name] = d / mmax
-    del states
+        torch.cuda.empty_cache()
+    del qref
     torch.cuda.empty_cache()
-    rate = lambda ms: lmx * 4 / (ms * 1e-3) / 1e6
-    return {"workload": "taylor_green_512^3, GCBC non-reflective x faces, periodic y/z",
-            "plain": dict(out[0], value=rate(out[0]["ms_per_step"])),
-            "mixed": dict(out[1], value=rate(out[1]["ms_per_step"])),
-            "speedup_mixed_vs_plain": out[0]["ms_per_step"] / out[1]["ms_per_step"],
-            "mixed_refinement_sweep_on": dict(out[2], value=rate(out[2]["ms_per_step"]),
-                                              speedup_vs_plain=out[0]["ms_per_step"] / out[2]["ms_per_step"]),
-            "rel_err_mixed_vs_fp64_per_field": errs,
-            "rel_err_momentum_vs_max_momentum": errs_m, "steps_compared": steps + 1, "unit": UNIT}
+    return dict(out, workload="taylor_green_512^3, GCBC non-reflective x faces, periodic y/z",
+                speedup_mixed_vs_plain=out["plain"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+                steps_compared=steps + 1, unit=UNIT)
 
 
 CURV_STAGE_BYTES = 864 + 3 * 80 + 80 // 4  # + metrics in the 3 flux passes and the dt pass of stage 0
@@ -902,59 +913,59 @@ def run_ours(args):
     # --- mixed form: same workload and timing, error against the FP64 path -------
     mixed = None
     if not args.no_mixed:
-        sm = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, precision=1))
-        qm = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
-        cs.tgv_init(qm, dims, MACH, 1e-4, rank)
-        qp = qm.clone()
-        for _ in range(args.warmup):
-            sm.step(qm, 0.0)
-        barrier(world)
-        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        g0.record(stream)
-        for _ in range(args.steps):
-            sm.step(qm, 0.0)
-        g1.record(stream)
-        barrier(world)
-        tm_ms = max_over_ranks(g0.elapsed_time(g1), world)
-        # accuracy: W + K steps of each form from the same initial state
-        for _ in range(args.steps + args.warmup):
+        # the mixed forms, each autotuned, timed like `value`; state error
+        # against the FP64 path after 100 steps from the same initial state
+        from compact_schemes_b200.solver import PREC_MIXED, PREC_MIXED_F32, REFINE_ALL
+        acc_steps = 100
+        qp = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
+        cs.tgv_init(qp, dims, MACH, 1e-4, rank)
+        for _ in range(acc_steps):
             s.step(qp, 0.0)
-        torch.cuda.synchronize()
-        errs = [float((qm[i * lmx:(i + 1) * lmx] - qp[i * lmx:(i + 1) * lmx]).abs().max() /
-                      qp[i * lmx:(i + 1) * lmx].abs().max()) for i in range(5)]
-        mmax = max(float(qp[i * lmx:(i + 1) * lmx].abs().max()) for i in (1, 2, 3))
-        errs_m = {n_: float((qm[i * lmx:(i + 1) * lmx] - qp[i * lmx:(i + 1) * lmx]).abs().max()) / mmax
-                  for i, n_ in ((1, "rho_u"), (2, "rho_v"), (3, "rho_w"))}
-        mvalue = world * pts_stages_per_step * args.steps / (tm_ms * 1e-3) / 1e6
-        # the same form with the FP64-residual refinement sweep after every FP32 solve
-        from compact_schemes_b200.solver import REFINE_ALL
-        sr = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, precision=1, refine=REFINE_ALL))
-        qr = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
-        cs.tgv_init(qr, dims, MACH, 1e-4, rank)
-        for _ in range(args.warmup):
-            sr.step(qr, 0.0)
-        barrier(world)
-        g0.record(stream)
-        for _ in range(args.steps):
-            sr.step(qr, 0.0)
-        g1.record(stream)
-        barrier(world)
-        tr_ms = max_over_ranks(g0.elapsed_time(g1), world)
-        errs_r = [float((qr[i * lmx:(i + 1) * lmx] - qp[i * lmx:(i + 1) * lmx]).abs().max() /
-                        qp[i * lmx:(i + 1) * lmx].abs().max()) for i in range(5)]
-        sr.close()
-        del qr
-        mixed = {"value": mvalue, "unit": UNIT, "ms_per_step": tm_ms / args.steps,
-                 "speedup_vs_plain": mvalue / value,
-                 "refinement_sweep_on": {"ms_per_step": tr_ms / args.steps, "speedup_vs_plain": t_ms / tr_ms,
-                                         "rel_err_vs_fp64_per_field":
-                                             dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_E"], errs_r))},
-                 "rel_err_vs_fp64_per_field": dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_E"], errs)),
-                 "rel_err_momentum_vs_max_momentum": errs_m,
-                 "steps_compared": args.steps + args.warmup,
-                 "arith": "FP32 fluxes/line solves; FP64 state, RK, thermo, RHS rows; no refinement sweep"}
-        sm.close()
-        del qm, qp
+        variants = [("mixed", PREC_MIXED_F32, 0), ("mixed_fp64_rhs", PREC_MIXED, 0),
+                    ("refinement_sweep_on", PREC_MIXED, REFINE_ALL)]
+        res = {}
+        for key, prec, refine in variants:
+            sm = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, precision=prec,
+                                         refine=refine))
+            qm = torch.empty(5 * lmx, dtype=torch.float64, device="cuda")
+            cs.tgv_init(qm, dims, MACH, 1e-4, rank)
+            choice = sm.autotune(qm, reps=1)
+            for _ in range(args.warmup):
+                sm.step(qm, 0.0)
+            barrier(world)
+            g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            g0.record(stream)
+            for _ in range(args.steps):
+                sm.step(qm, 0.0)
+            g1.record(stream)
+            barrier(world)
+            tm_ms = max_over_ranks(g0.elapsed_time(g1), world)
+            cs.tgv_init(qm, dims, MACH, 1e-4, rank)
+            for _ in range(acc_steps):
+                sm.step(qm, 0.0)
+            torch.cuda.synchronize()
+            errs, errs_m = state_errors(qm, qp, lmx)
+            mvalue = world * pts_stages_per_step * args.steps / (tm_ms * 1e-3) / 1e6
+            res[key] = {"value": mvalue, "unit": UNIT, "ms_per_step": tm_ms / args.steps,
+                        "speedup_vs_plain": mvalue / value,
+                        "schedule": {"%s_%s" % ("grad" if k == 0 else "flux", "xyz"[a]): v
+                                     for (k, a), v in choice.items()},
+                        "rel_err_vs_fp64_per_field": errs, "rel_err_momentum_vs_max_momentum": errs_m,
+                        "steps_compared": acc_steps}
+            sm.close()
+            del qm
+            torch.cuda.empty_cache()
+        del qp
+        mixed = dict(res["mixed"],
+                     arith="FP32 fluxes, interior right-hand sides and line solves (per-row factors as "
+                           "constants); FP64 state, RK accumulation, thermodynamics and closure rows; "
+                           "no refinement sweep",
+                     mixed_fp64_rhs=dict(res["mixed_fp64_rhs"],
+                                         arith="fluxes and every right-hand side formed in FP64, FP32 line "
+                                               "solves from tables"),
+                     refinement_sweep_on=dict(res["refinement_sweep_on"],
+                                              arith="mixed_fp64_rhs plus one FP64-residual refinement sweep "
+                                                    "after every FP32 line solve"))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
