@@ -130,6 +130,16 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
 #ifndef CSB_CF_SOLVE_GROUP
 #define CSB_CF_SOLVE_GROUP 2
 #endif
+// resident 256-thread CTAs per SM asked of the compiler (register cap) for
+// the mixed one-phase flux passes with ChunkFactors (measured at 256^3: three
+// CTAs per SM cut the x / y flux passes from 0.31 / 0.50 to 0.25 / 0.41 ms),
+// and points per thread loaded together in their load phase
+#ifndef CSB_MX_FLUX_MINB
+#define CSB_MX_FLUX_MINB 3
+#endif
+#ifndef CSB_MX_FLUX_UNROLL
+#define CSB_MX_FLUX_UNROLL CSB_FLUX_UNROLL
+#endif
 
 // FP32 solve of G lines with ChunkFactors (interface closure on both ends,
 // full chunks): interior right-hand sides in FP32, the four closure rows of
@@ -405,7 +415,7 @@ __device__ __forceinline__ void point_flux_f32(const float *__restrict__ sh, con
 }
 
 template <int LT, int AXIS, int TL, int MODE, bool VISC, bool SHADOW_OUT, bool REF, bool CF = false>
-__global__ void __launch_bounds__(TL * 32, TL == 8 ? 2 : 1)
+__global__ void __launch_bounds__(TL * 32, TL == 8 ? (CF ? CSB_MX_FLUX_MINB : 2) : 1)
 k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__restrict__ rhs,
           const double *__restrict__ qn, double *__restrict__ qout, float *__restrict__ sh_out,
           double *__restrict__ drva, DevTables<float> tab, int lxi, int let, int64_t lmx, int64_t F,
@@ -417,7 +427,7 @@ k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__re
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t line0 = (int64_t)blockIdx.x * TL;
     const PhysF pf = phys_f32(ph);
-    tile_for_each<AXIS, TL, CSB_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
+    tile_for_each<AXIS, TL, CSB_MX_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         float fl[5];
         if (CF) point_flux_f32<AXIS, VISC>(sh, g, lmx, gi, pf, fl);
         else point_flux_mx<AXIS, VISC>(sh, g, lmx, gi, ph, fl);
