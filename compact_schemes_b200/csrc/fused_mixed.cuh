@@ -131,7 +131,8 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
 #define CSB_CF_SOLVE_GROUP 2
 #endif
 // resident 256-thread CTAs per SM asked of the compiler (register cap) for
-// the mixed one-phase flux passes with ChunkFactors (measured at 256^3: three
+// the mixed one-phase flux passes with ChunkFactors and no refinement sweep
+// (with the sweep they would spill; measured at 256^3: three
 // CTAs per SM cut the x / y flux passes from 0.31 / 0.50 to 0.25 / 0.41 ms),
 // and points per thread loaded together in their load phase
 #ifndef CSB_MX_FLUX_MINB
@@ -144,8 +145,12 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
 // FP32 solve of G lines with ChunkFactors (interface closure on both ends,
 // full chunks): interior right-hand sides in FP32, the four closure rows of
 // each line in FP64 (group_closure_rows), per-row factors from the kernel
-// parameters.  The results overwrite the lines.
-template <int LT, int G>
+// parameters.  REF adds one refinement sweep: the residual r - A x of the
+// FP32 right-hand side r and solution x is formed in FP64 (rows
+// alpha x[j-1] + x[j] + alpha x[j+1], with no coupling outside the line),
+// rounded once, solved in FP32 and added to x.  The results overwrite the
+// lines.
+template <int LT, int G, bool REF = false>
 __device__ __forceinline__ void solve_lines_cf(float *const (&lines)[G], int nf, int lane,
                                                const DevTables<float> &tab, const ChunkFactors<LT> &U,
                                                const Coeffs &cf) {
@@ -162,7 +167,36 @@ __device__ __forceinline__ void solve_lines_cf(float *const (&lines)[G], int nf,
             for (int t = 0; t < LT; ++t) x[g][t] = 0.0f;
         }
     }
-    warp_solve_cf<LT, G>(U, tab, x, lane);
+    if (REF) {
+        float r[G][LT];
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int t = 0; t < LT; ++t) r[g][t] = x[g][t];
+        warp_solve_cf<LT, G>(U, tab, x, lane);
+        const bool first = lane == 0, last = lane == p - 1, live = lane < p;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const double xm0 = (double)__shfl_up_sync(0xffffffffu, x[g][LT - 1], 1);
+            const double xp0 = (double)__shfl_down_sync(0xffffffffu, x[g][0], 1);
+            double xm = first ? 0.0 : xm0, xc = (double)x[g][0];
+#pragma unroll
+            for (int t = 0; t < LT; ++t) {
+                const double xp = t + 1 < LT ? (double)x[g][t + 1] : (last ? 0.0 : xp0);
+                const double res = (double)r[g][t] - fma(kAlpha, xm + xp, xc);
+                r[g][t] = live ? (float)res : 0.0f;
+                xm = xc;
+                xc = xp;
+            }
+        }
+        warp_solve_cf<LT, G>(U, tab, r, lane);
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int t = 0; t < LT; ++t) x[g][t] += r[g][t];
+    } else {
+        warp_solve_cf<LT, G>(U, tab, x, lane);
+    }
     __syncwarp();
 #pragma unroll
     for (int g = 0; g < G; ++g) {
@@ -177,19 +211,19 @@ __device__ __forceinline__ void solve_lines_cf(float *const (&lines)[G], int nf,
 // The NF fields of this warp's line of the tile, CSB_MX_SOLVE_GROUP at a time
 // (one at a time for lines of more than 256 points when the refinement sweep
 // is compiled in: registers).
-// CF: the lines have ChunkFactors (solve_lines_cf; no refinement sweep).
+// CF: the lines have ChunkFactors (solve_lines_cf, with the sweep if REF).
 template <int LT, int TL, int NF, bool REF, bool CF = false>
 __device__ __forceinline__ void solve_fields_mx(float *sm, int w, int lane, const DevTables<float> &tab,
                                                 int nstart, int nend, const Coeffs &cf,
                                                 const ChunkFactors<LT> &U) {
     if (CF) {
-        constexpr int G = CSB_CF_SOLVE_GROUP;
+        constexpr int G = REF && LT >= 16 ? 1 : CSB_CF_SOLVE_GROUP;
 #pragma unroll 1
         for (int c = 0; c < NF; c += G) {
             float *lines[G];
 #pragma unroll
             for (int g = 0; g < G; ++g) lines[g] = field_line32<LT, TL>(sm, c + g < NF ? c + g : c, w);
-            solve_lines_cf<LT, G>(lines, NF - c, lane, tab, U, cf);
+            solve_lines_cf<LT, G, REF>(lines, NF - c, lane, tab, U, cf);
         }
         return;
     }
@@ -415,7 +449,7 @@ __device__ __forceinline__ void point_flux_f32(const float *__restrict__ sh, con
 }
 
 template <int LT, int AXIS, int TL, int MODE, bool VISC, bool SHADOW_OUT, bool REF, bool CF = false>
-__global__ void __launch_bounds__(TL * 32, TL == 8 ? (CF ? CSB_MX_FLUX_MINB : 2) : 1)
+__global__ void __launch_bounds__(TL * 32, TL == 8 ? (CF && !REF ? CSB_MX_FLUX_MINB : 2) : 1)
 k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__restrict__ rhs,
           const double *__restrict__ qn, double *__restrict__ qout, float *__restrict__ sh_out,
           double *__restrict__ drva, DevTables<float> tab, int lxi, int let, int64_t lmx, int64_t F,
@@ -518,9 +552,9 @@ struct MixedArgs {
     int fp32;       // FP32 interior arithmetic where the line has ChunkFactors
 };
 
-// The pass runs the ChunkFactors kernels: FP32 interior arithmetic asked for,
-// no refinement sweep, and the line's tables uniform.
-inline bool use_cf(const MixedArgs &a) { return a.fp32 && !a.refine && a.base.tab->uniform; }
+// The pass runs the ChunkFactors kernels: FP32 interior arithmetic asked for
+// and the line's tables uniform (the refinement sweep, if on, is theirs).
+inline bool use_cf(const MixedArgs &a) { return a.fp32 && a.base.tab->uniform; }
 
 template <int LT>
 ChunkFactors<LT> chunk_factors_of(const DeviceTables &dt) {
@@ -541,9 +575,9 @@ template <int LT, int AXIS, int TL>
 int launch_grad_mx_t(const MixedArgs &a, const double *q, bool first, cudaStream_t st) {
     const size_t smem = (size_t)4 * TL * LineLayout<LT>::kSlot * sizeof(float);
     const bool cfp = use_cf(a);
-    auto kern = first ? (a.refine ? k_grad_mx<LT, AXIS, TL, true, true>
+    auto kern = first ? (a.refine ? (cfp ? k_grad_mx<LT, AXIS, TL, true, true, true> : k_grad_mx<LT, AXIS, TL, true, true>)
                                   : (cfp ? k_grad_mx<LT, AXIS, TL, true, false, true> : k_grad_mx<LT, AXIS, TL, true, false>))
-                      : (a.refine ? k_grad_mx<LT, AXIS, TL, false, true>
+                      : (a.refine ? (cfp ? k_grad_mx<LT, AXIS, TL, false, true, true> : k_grad_mx<LT, AXIS, TL, false, true>)
                                   : (cfp ? k_grad_mx<LT, AXIS, TL, false, false, true>
                                          : k_grad_mx<LT, AXIS, TL, false, false>));
     if (int rc = set_smem(kern, smem)) return rc;
@@ -571,9 +605,9 @@ int launch_flux_mx_t(const MixedArgs &a, const double *qn, double *qout, bool sh
                          : (shadow_out && kRk ? k_flux_mx<LT, AXIS, TL, MODE, false, kRk, R, C>
                                               : k_flux_mx<LT, AXIS, TL, MODE, false, false, R, C>);
     };
-    auto kern = a.refine ? pick(std::true_type{}, std::false_type{})
-                         : (use_cf(a) ? pick(std::false_type{}, std::true_type{})
-                                      : pick(std::false_type{}, std::false_type{}));
+    const bool cfp = use_cf(a);
+    auto kern = a.refine ? (cfp ? pick(std::true_type{}, std::true_type{}) : pick(std::true_type{}, std::false_type{}))
+                         : (cfp ? pick(std::false_type{}, std::true_type{}) : pick(std::false_type{}, std::false_type{}));
     if (int rc = set_smem(kern, smem)) return rc;
     const unsigned blocks = (unsigned)((b.F + TL - 1) / TL);
     kern<<<blocks, TL * 32, smem, st>>>(a.shadow, a.grad, a.rhs, qn, qout, a.shadow, drva, b.tab->t32, b.lxi,

@@ -144,44 +144,47 @@ __device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][L
 // kernel's parameters, so the solve reads them as constants instead of
 // loading six per-lane table entries per row.  nra / nrc are the negated
 // spike coefficients (rca / rcc of the tables).
-template <int LT>
+template <int LT, typename CT = float>
 struct ChunkFactors {
-    float f1[LT], f2[LT], b1[LT], b2[LT], nra[LT], nrc[LT];
+    CT f1[LT], f2[LT], b1[LT], b2[LT], nra[LT], nrc[LT];
 };
 
+__device__ __forceinline__ float cf_fma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double cf_fma(double a, double b, double c) { return fma(a, b, c); }
+
 // warp_solve for lines with ChunkFactors (all chunks full, no cyclic
-// correction): FP32, NV right-hand sides held as d[v][t].  The structure of
-// the tables fixes fwd2 = 0 for rows 0 and 1 of a chunk, bwd1 = 1 and bwd2 = 0
-// for row LT - 2, and bwd1 = 1 for rows 1 .. LT - 3; those products are
-// left out.  All 32 lanes must call it.
-template <int LT, int NV>
-__device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT> &U, const DevTables<float> &T,
-                                              float (&d)[NV][LT], int lane) {
+// correction): NV right-hand sides held as d[v][t], FP32 or FP64.  The
+// structure of the tables fixes fwd2 = 0 for rows 0 and 1 of a chunk, bwd1 = 1
+// and bwd2 = 0 for row LT - 2, and bwd1 = 1 for rows 1 .. LT - 3; those
+// products are left out.  All 32 lanes must call it.
+template <int LT, int NV, typename CT>
+__device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT, CT> &U, const DevTables<CT> &T,
+                                              CT (&d)[NV][LT], int lane) {
     static_assert(LT >= 2, "chunk");
 #pragma unroll
     for (int t = 0; t < LT; ++t)
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-            d[v][t] = t < 2 ? U.f1[t] * d[v][t] : fmaf(U.f2[t], d[v][t - 1], U.f1[t] * d[v][t]);
+            d[v][t] = t < 2 ? U.f1[t] * d[v][t] : cf_fma(U.f2[t], d[v][t - 1], U.f1[t] * d[v][t]);
 #pragma unroll
     for (int t = LT - 3; t >= 0; --t)
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-            d[v][t] = t == 0 ? fmaf(U.b2[0], d[v][1], U.b1[0] * d[v][0]) : fmaf(U.b2[t], d[v][t + 1], d[v][t]);
-    float y0[NV], y1[NV];
+            d[v][t] = t == 0 ? cf_fma(U.b2[0], d[v][1], U.b1[0] * d[v][0]) : cf_fma(U.b2[t], d[v][t + 1], d[v][t]);
+    CT y0[NV], y1[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         y0[v] = d[v][0];
         y1[v] = d[v][LT - 1];
     }
     {
-        const float ka = T.k1[lane], kb = T.k2[lane], kc = T.k1[32 + lane], kd = T.k2[32 + lane];
+        const CT ka = T.k1[lane], kb = T.k2[lane], kc = T.k1[32 + lane], kd = T.k2[32 + lane];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const float up1 = __shfl_up_sync(0xffffffffu, y1[v], 1);
-            const float dn0 = __shfl_down_sync(0xffffffffu, y0[v], 1);
-            const float n0 = y0[v] - ka * up1 - kb * y1[v];
-            const float n1 = y1[v] - kc * y0[v] - kd * dn0;
+            const CT up1 = __shfl_up_sync(0xffffffffu, y1[v], 1);
+            const CT dn0 = __shfl_down_sync(0xffffffffu, y0[v], 1);
+            const CT n0 = y0[v] - ka * up1 - kb * y1[v];
+            const CT n1 = y1[v] - kc * y0[v] - kd * dn0;
             y0[v] = n0;
             y1[v] = n1;
         }
@@ -190,25 +193,25 @@ __device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT> &U, const D
     for (int s = 1; s < kPcrSteps; ++s) {
         if (s >= T.pcr) break;
         const int dl = 1 << (s - 1);
-        const float ka = T.k1[s * 64 + lane], kb = T.k2[s * 64 + lane];
-        const float kc = T.k1[s * 64 + 32 + lane], kd = T.k2[s * 64 + 32 + lane];
+        const CT ka = T.k1[s * 64 + lane], kb = T.k2[s * 64 + lane];
+        const CT kc = T.k1[s * 64 + 32 + lane], kd = T.k2[s * 64 + 32 + lane];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const float u0 = __shfl_up_sync(0xffffffffu, y0[v], dl);
-            const float d0 = __shfl_down_sync(0xffffffffu, y0[v], dl);
-            const float u1 = __shfl_up_sync(0xffffffffu, y1[v], dl);
-            const float d1 = __shfl_down_sync(0xffffffffu, y1[v], dl);
+            const CT u0 = __shfl_up_sync(0xffffffffu, y0[v], dl);
+            const CT d0 = __shfl_down_sync(0xffffffffu, y0[v], dl);
+            const CT u1 = __shfl_up_sync(0xffffffffu, y1[v], dl);
+            const CT d1 = __shfl_down_sync(0xffffffffu, y1[v], dl);
             y0[v] = y0[v] - ka * u0 - kb * d0;
             y1[v] = y1[v] - kc * u1 - kd * d1;
         }
     }
-    const float ib0 = T.invb[lane], ib1 = T.invb[32 + lane];
+    const CT ib0 = T.invb[lane], ib1 = T.invb[32 + lane];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        const float X0 = y0[v] * ib0, X1 = y1[v] * ib1;
+        const CT X0 = y0[v] * ib0, X1 = y1[v] * ib1;
         d[v][0] = X0;
 #pragma unroll
-        for (int t = 1; t + 1 < LT; ++t) d[v][t] = fmaf(U.nrc[t], X1, fmaf(U.nra[t], X0, d[v][t]));
+        for (int t = 1; t + 1 < LT; ++t) d[v][t] = cf_fma(U.nrc[t], X1, cf_fma(U.nra[t], X0, d[v][t]));
         d[v][LT - 1] = X1;
     }
 }

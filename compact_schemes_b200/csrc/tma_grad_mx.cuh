@@ -18,8 +18,8 @@
 //   3. one thread refills the staging buffer with tile k + 2;
 //   4. each warp solves its fields of one line in place: the FP32 interior
 //      form with per-row constants (solve_lines_cf) where the line has
-//      ChunkFactors, else the table form (solve_lines_mx, refinement sweep
-//      as configured);
+//      ChunkFactors, else the table form (solve_lines_mx); either with the
+//      refinement sweep when it is on;
 //   5. the four derivatives go to HBM with coalesced stores.
 // The arithmetic is that of k_grad_mx with the same solve: results are
 // bit-identical to it.  Boxes that reach past the end of the array read zeros
@@ -37,7 +37,8 @@ constexpr int tma_mx_tile() {
     return LT <= 8 ? 8 : 4;
 }
 
-// MODE: 0 table solve, 1 table solve with the refinement sweep, 2 ChunkFactors.
+// MODE: 0 table solve, 1 table solve with the refinement sweep, 2 ChunkFactors,
+// 3 ChunkFactors with the refinement sweep.
 template <int LT, int AXIS, int MODE>
 __global__ void __launch_bounds__(256, 2)
 k_grad_mx_tma(const __grid_constant__ CUtensorMap smap, float *__restrict__ g, DevTables<float> tab, TmaGeom geo,
@@ -46,7 +47,7 @@ k_grad_mx_tma(const __grid_constant__ CUtensorMap smap, float *__restrict__ g, D
     constexpr int TL = tma_mx_tile<LT>();
     constexpr int NT = 256;
     constexpr int FPW = 4 * TL / (NT / 32);  // fields per warp: 4 (TL 8) or 2 (TL 4)
-    constexpr int G = MODE == 1 && LT >= 16 ? 1 : 2;
+    constexpr int G = (MODE == 1 || MODE == 3) && LT >= 16 ? 1 : 2;
     using L = LineLayout<LT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int stage_elems = geo.nbox * 4 * TL * geo.boxlen;
@@ -128,7 +129,7 @@ k_grad_mx_tma(const __grid_constant__ CUtensorMap smap, float *__restrict__ g, D
                     float *lines[G];
 #pragma unroll
                     for (int gg = 0; gg < G; ++gg) lines[gg] = field_line32<LT, TL>(solve, c + gg, l);
-                    if (MODE == 2) solve_lines_cf<LT, G>(lines, G, lane, tab, U, cf);
+                    if (MODE >= 2) solve_lines_cf<LT, G, MODE == 3>(lines, G, lane, tab, U, cf);
                     else solve_lines_mx<LT, G, MODE == 1>(lines, G, lane, tab, nstart, nend, cf, MODE == 1 ? 1 : 0);
                 }
             }
@@ -158,7 +159,8 @@ int launch_grad_mx_tma_t(const MixedArgs &a, const cs_dcomp &d, int *err, cudaSt
         return set_error(CS_ERR_UNSUPPORTED, "mixed TMA gradient pass: unsupported geometry");
     CUtensorMap map;
     if (int rc = tma_field_map32(AXIS, d, tma_mx_tile<LT>(), geo.boxlen, 4, a.shadow + b.lmx, map)) return rc;
-    auto kern = a.refine ? k_grad_mx_tma<LT, AXIS, 1> : (use_cf(a) ? k_grad_mx_tma<LT, AXIS, 2> : k_grad_mx_tma<LT, AXIS, 0>);
+    auto kern = use_cf(a) ? (a.refine ? k_grad_mx_tma<LT, AXIS, 3> : k_grad_mx_tma<LT, AXIS, 2>)
+                          : (a.refine ? k_grad_mx_tma<LT, AXIS, 1> : k_grad_mx_tma<LT, AXIS, 0>);
     if (int rc = set_smem(kern, smem)) return rc;
     int per = 0;
     CSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, smem));

@@ -264,8 +264,9 @@ typedef struct cs_solver cs_solver;
                                evaluated in FP32, interior right-hand sides in FP32 (closure
                                rows in FP64) and per-row solver factors as constants, on every
                                axis whose lines have uniform chunk factors (interface or periodic
-                               closure, length a multiple of the chunk) and no refinement sweep;
-                               other axes run as CS_PREC_MIXED */
+                               closure, length a multiple of the chunk); cfg.refine adds the
+                               FP64-residual sweep of the FP32 right-hand side; other axes run
+                               as CS_PREC_MIXED */
 
 #define CS_REFINE_NONE 0 /* mixed: no refinement sweep */
 #define CS_REFINE_ALL 1  /* mixed: a refinement sweep after every FP32 line solve */

@@ -30,7 +30,8 @@ def make(dims, precision, **kw):
 
 
 @pytest.mark.parametrize("prec,refine,dims", [(1, 1, (48, 40, 32)), (1, 0, (48, 40, 32)), (1, 2, (48, 40, 32)),
-                                               (2, 0, (48, 40, 32)), (2, 0, (50, 33, 36))])
+                                               (2, 0, (48, 40, 32)), (2, 0, (50, 33, 36)), (2, 1, (48, 40, 32)),
+                                               (2, 1, (50, 33, 36))])
 def test_mixed_rhs_vs_oracle(cuda, prec, refine, dims):
     """Mixed RHS against the FP64 oracle, relative to the size of the summed terms
     (33-point lines are not a multiple of their chunk: that axis runs as precision 1)."""
@@ -46,7 +47,7 @@ def test_mixed_rhs_vs_oracle(cuda, prec, refine, dims):
     assert err < 2e-6, err
 
 
-@pytest.mark.parametrize("prec,refine", [(1, 0), (1, 1), (1, 2), (2, 0)])
+@pytest.mark.parametrize("prec,refine", [(1, 0), (1, 1), (1, 2), (2, 0), (2, 1)])
 def test_mixed_100_steps_within_1e6(cuda, prec, refine):
     import torch
     import compact_schemes_b200 as cs
@@ -95,14 +96,15 @@ def test_mixed_512_gcbc_100_steps(cuda, prec):
     assert errs[3] <= 1e-4, errs
 
 
-@pytest.mark.parametrize("prec,refine", [(1, 0), (1, 1), (2, 0)])
+@pytest.mark.parametrize("prec,refine", [(1, 0), (1, 1), (2, 0), (2, 1)])
 @pytest.mark.parametrize("dims,gcbc", [((64, 64, 64), False), ((40, 36, 300), False), ((36, 28, 20), True),
                                        ((48, 40, 1), False)])
 def test_mixed_tma_schedule_bit_identical(cuda, prec, refine, dims, gcbc):
     """The TMA-staged gradient passes of the mixed form (every gradient pass
     but a step's first) do the one-phase passes' arithmetic: RHS and three
     CFL-stepped RK steps agree bit for bit, for the table solve with and
-    without the refinement sweep and for the ChunkFactors solve.  The cases
+    without the refinement sweep and for the ChunkFactors solve with and
+    without it.  The cases
     cover 300-point z lines (two boxes per line, 4-line tiles), y tiles that
     overhang the x extent (36 = 4 tiles of 8 + 4), two active axes and GCBC
     x faces (table solve along x, ChunkFactors along y and z)."""
