@@ -89,17 +89,17 @@ def mixed_512_gcbc_section(args, steps=6):
     of each mixed state against the FP64 state after the same steps from the
     same initial state.  `mixed` is the FP32-interior form (CS_PREC_MIXED_F32:
     its x lines have physical closures and run the table solve; y and z the
-    ChunkFactors solve); `mixed_fp64_rhs` forms every right-hand side and flux
-    in FP64 (CS_PREC_MIXED); `mixed_refinement_sweep_on` adds the FP64-residual
-    refinement sweep to the latter."""
+    ChunkFactors solve); `mixed_refinement_sweep_on` adds the FP64-residual
+    refinement sweep to it; `mixed_fp64_rhs` forms every right-hand side and
+    flux in FP64 (CS_PREC_MIXED)."""
     import torch
     import compact_schemes_b200 as cs
     from compact_schemes_b200.solver import PREC_MIXED, PREC_MIXED_F32, REFINE_ALL
     n = 512
     lmx = n ** 3
     nbc = [[cs.BC_NON_REFLECTIVE, cs.BC_PERIODIC, cs.BC_PERIODIC]] * 2
-    variants = [("plain", 0, 0), ("mixed", PREC_MIXED_F32, 0), ("mixed_fp64_rhs", PREC_MIXED, 0),
-                ("mixed_refinement_sweep_on", PREC_MIXED, REFINE_ALL)]
+    variants = [("plain", 0, 0), ("mixed", PREC_MIXED_F32, 0), ("mixed_refinement_sweep_on", PREC_MIXED_F32, REFINE_ALL),
+                ("mixed_fp64_rhs", PREC_MIXED, 0)]
     out, qref = {}, None
     for key, prec, refine in variants:
         s = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, nbc=nbc, gcbc=True,
@@ -921,8 +921,8 @@ def run_ours(args):
         cs.tgv_init(qp, dims, MACH, 1e-4, rank)
         for _ in range(acc_steps):
             s.step(qp, 0.0)
-        variants = [("mixed", PREC_MIXED_F32, 0), ("mixed_fp64_rhs", PREC_MIXED, 0),
-                    ("refinement_sweep_on", PREC_MIXED, REFINE_ALL)]
+        variants = [("mixed", PREC_MIXED_F32, 0), ("refinement_sweep_on", PREC_MIXED_F32, REFINE_ALL),
+                    ("mixed_fp64_rhs", PREC_MIXED, 0)]
         res = {}
         for key, prec, refine in variants:
             sm = cs.Solver(cs.tgv_config(n, mach=MACH, re=RE, cfl=CFL, use_graph=True, precision=prec,
@@ -964,8 +964,9 @@ def run_ours(args):
                                          arith="fluxes and every right-hand side formed in FP64, FP32 line "
                                                "solves from tables"),
                      refinement_sweep_on=dict(res["refinement_sweep_on"],
-                                              arith="mixed_fp64_rhs plus one FP64-residual refinement sweep "
-                                                    "after every FP32 line solve"))
+                                              arith="mixed plus one refinement sweep after every FP32 line "
+                                                    "solve: residual of the FP32 right-hand side formed in FP64, "
+                                                    "solved in FP32, added"))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
