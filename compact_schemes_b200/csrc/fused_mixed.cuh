@@ -552,9 +552,14 @@ struct MixedArgs {
     int fp32;       // FP32 interior arithmetic where the line has ChunkFactors
 };
 
-// The pass runs the ChunkFactors kernels: FP32 interior arithmetic asked for
+// The pass runs the ChunkFactors kernels: FP32 interior arithmetic asked for,
+// the interface closure on both ends (deriv_rhs_cf forms those closure rows)
 // and the line's tables uniform (the refinement sweep, if on, is theirs).
-inline bool use_cf(const MixedArgs &a) { return a.fp32 && a.base.tab->uniform; }
+// Uniform tables alone do not imply the interface closure: with 2-row chunks
+// the physical closure's rows only enter the reduced system.
+inline bool use_cf(const MixedArgs &a) {
+    return a.fp32 && a.base.nstart && a.base.nend && a.base.tab->uniform;
+}
 
 template <int LT>
 ChunkFactors<LT> chunk_factors_of(const DeviceTables &dt) {

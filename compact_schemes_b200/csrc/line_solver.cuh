@@ -33,6 +33,9 @@ struct DevTables {
     CT cyc_s1, cyc_s2;
     int n, p, last_len, cyclic;
     int pcr;  // PCR steps run on the reduced system (2..6)
+    // every lane's per-row factors (fwd1 .. rcc) equal interior_chunk<LT>'s:
+    // warp_solve then takes them as compile-time constants
+    int interior;
 };
 
 // Shared-memory layout of one line: element j = c*LT + t lives at
@@ -54,10 +57,67 @@ __device__ __forceinline__ int lane_len(int lane, int lt, int p, int last_len) {
     return lane < p - 1 ? lt : (lane == p - 1 ? last_len : 0);
 }
 
+// Per-row factors of one full chunk of LT rows of the constant interior rows
+// (alpha, 1, alpha) of the compact derivative, computed at compile time with
+// the operations and operation order of build_tables (tables.cpp), so that
+// they equal the tables of any line whose every chunk is such a chunk (the
+// interface / periodic closure with n a multiple of LT; the host checks the
+// equality before it sets DevTables::interior).
+template <int LT>
+struct InteriorChunk {
+    double fwd1[LT], fwd2[LT], bwd1[LT], bwd2[LT], rca[LT], rcc[LT];
+};
+template <int LT>
+__host__ __device__ constexpr InteriorChunk<LT> interior_chunk() {
+    InteriorChunk<LT> k{};
+    double A[LT] = {}, C[LT] = {};
+    const double a = kAlpha, b = 1.0, c = kAlpha;
+    for (int t = 0; t < LT; ++t) {
+        k.bwd1[t] = 1.0;
+        if (t < 2) {
+            k.fwd1[t] = 1.0 / b;
+            k.fwd2[t] = 0.0;
+            A[t] = a / b;
+            C[t] = c / b;
+        } else {
+            const double r = 1.0 / (b - a * C[t - 1]);
+            k.fwd1[t] = r;
+            k.fwd2[t] = -r * a;
+            A[t] = -r * a * A[t - 1];
+            C[t] = r * c;
+        }
+    }
+    if (LT >= 3) {
+        for (int t = LT - 3; t >= 1; --t) {
+            k.bwd1[t] = 1.0;
+            k.bwd2[t] = -C[t];
+            A[t] = A[t] - C[t] * A[t + 1];
+            C[t] = -C[t] * C[t + 1];
+        }
+        const double r = 1.0 / (1.0 - C[0] * A[1]);
+        k.bwd1[0] = r;
+        k.bwd2[0] = -r * C[0];
+        A[0] = r * A[0];
+        C[0] = -r * C[0] * C[1];
+    }
+    for (int t = 1; t + 1 < LT; ++t) {
+        k.rca[t] = A[t];
+        k.rcc[t] = C[t];
+    }
+    return k;
+}
+
+template <int LT, int NV, typename CT>
+__device__ __forceinline__ void warp_solve_interior(const DevTables<CT> &T, CT (&d)[NV][LT], int lane);
+
 // Solve NV right-hand sides held as d[v][t] by the lanes of one warp; the
 // solution overwrites d.  All 32 lanes must call it (warp shuffles).
 template <int LT, int NV, typename CT>
 __device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][LT], int lane) {
+    if (LT >= 2 && T.interior) {
+        warp_solve_interior<LT, NV, CT>(T, d, lane);
+        return;
+    }
     const int len = lane_len(lane, LT, T.p, T.last_len);
 #pragma unroll
     for (int t = 0; t < LT; ++t) {
@@ -213,6 +273,26 @@ __device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT, CT> &U, con
 #pragma unroll
         for (int t = 1; t + 1 < LT; ++t) d[v][t] = cf_fma(U.nrc[t], X1, cf_fma(U.nra[t], X0, d[v][t]));
         d[v][LT - 1] = X1;
+    }
+}
+
+// warp_solve for tables flagged `interior`: the per-row factors are the
+// compile-time interior_chunk<LT> values.
+template <int LT, int NV, typename CT>
+__device__ __forceinline__ void warp_solve_interior(const DevTables<CT> &T, CT (&d)[NV][LT], int lane) {
+    if constexpr (LT >= 2) {
+        constexpr InteriorChunk<LT> K = interior_chunk<LT>();
+        ChunkFactors<LT, CT> U{};
+#pragma unroll
+        for (int t = 0; t < LT; ++t) {
+            U.f1[t] = (CT)K.fwd1[t];
+            U.f2[t] = (CT)K.fwd2[t];
+            U.b1[t] = (CT)K.bwd1[t];
+            U.b2[t] = (CT)K.bwd2[t];
+            U.nra[t] = (CT)(-K.rca[t]);
+            U.nrc[t] = (CT)(-K.rcc[t]);
+        }
+        warp_solve_cf<LT, NV, CT>(U, T, d, lane);
     }
 }
 

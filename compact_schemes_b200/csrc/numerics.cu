@@ -39,6 +39,32 @@ TableCache::~TableCache() {
     }
 }
 
+// Whether every lane's per-row factors equal the compile-time interior_chunk
+// values (exact comparison): the line's chunks are all full and hold only the
+// constant interior rows.
+template <int LT>
+static bool interior_match(const HostTables &h) {
+    constexpr InteriorChunk<LT> K = interior_chunk<LT>();
+    const std::vector<double> *tabs[6] = {&h.fwd1, &h.fwd2, &h.bwd1, &h.bwd2, &h.rca, &h.rcc};
+    const double *ref[6] = {K.fwd1, K.fwd2, K.bwd1, K.bwd2, K.rca, K.rcc};
+    for (int k = 0; k < 6; ++k)
+        for (int t = 0; t < LT; ++t)
+            for (int lane = 0; lane < h.p; ++lane)
+                if ((*tabs[k])[(size_t)t * 32 + lane] != ref[k][t]) return false;
+    return true;
+}
+static bool interior_tables(const HostTables &h) {
+    if (h.cyclic || h.n != h.p * h.lt || h.p < 2) return false;
+    switch (h.lt) {
+        case 2: return interior_match<2>(h);
+        case 4: return interior_match<4>(h);
+        case 8: return interior_match<8>(h);
+        case 16: return interior_match<16>(h);
+        case 32: return interior_match<32>(h);
+    }
+    return false;
+}
+
 template <typename CT>
 static void bind(DevTables<CT> &t, CT *base, const HostTables &h) {
     const size_t tl = (size_t)h.lt * 32;
@@ -59,6 +85,7 @@ static void bind(DevTables<CT> &t, CT *base, const HostTables &h) {
     t.last_len = h.last_len;
     t.cyclic = h.cyclic ? 1 : 0;
     t.pcr = sizeof(CT) == 4 ? h.pcr32 : h.pcr64;
+    t.interior = interior_tables(h) ? 1 : 0;
 }
 
 // Device layout of the tables; fp32 selects the inverse diagonals of the

@@ -29,16 +29,24 @@ def make(dims, precision, **kw):
     return cs.Solver(cs.tgv_config(None, dims=dims, precision=precision, **kw))
 
 
-@pytest.mark.parametrize("prec,refine,dims", [(1, 1, (48, 40, 32)), (1, 0, (48, 40, 32)), (1, 2, (48, 40, 32)),
-                                               (2, 0, (48, 40, 32)), (2, 0, (50, 33, 36)), (2, 1, (48, 40, 32)),
-                                               (2, 1, (50, 33, 36))])
-def test_mixed_rhs_vs_oracle(cuda, prec, refine, dims):
+@pytest.mark.parametrize("prec,refine,dims,xphys", [(1, 1, (48, 40, 32), 0), (1, 0, (48, 40, 32), 0),
+                                                     (1, 2, (48, 40, 32), 0), (2, 0, (48, 40, 32), 0),
+                                                     (2, 0, (50, 33, 36), 0), (2, 1, (48, 40, 32), 0),
+                                                     (2, 1, (50, 33, 36), 0), (2, 0, (36, 28, 20), 1),
+                                                     (2, 1, (36, 28, 20), 1), (1, 0, (36, 28, 20), 1)])
+def test_mixed_rhs_vs_oracle(cuda, prec, refine, dims, xphys):
     """Mixed RHS against the FP64 oracle, relative to the size of the summed terms
-    (33-point lines are not a multiple of their chunk: that axis runs as precision 1)."""
+    (33-point lines are not a multiple of their chunk: that axis runs as precision 1).
+    xphys: physical (non-reflective, no characteristic correction) closures on
+    the x faces; 36-point x lines have uniform 2-row chunk factors but no
+    interface closure, so they must run the table form."""
     import torch
+    import compact_schemes_b200 as cs
     q = O.tgv_init(dims, MACH, 1e-4, 0)
-    ref, scale = O.rhs(q, MU, O.uniform_metrics(*dims), dims, [[1] * 3, [1] * 3], with_scale=True)
-    s = make(dims, prec, refine=refine)
+    ndf = [[0 if xphys else 1, 1, 1]] * 2
+    ref, scale = O.rhs(q, MU, O.uniform_metrics(*dims), dims, ndf, with_scale=True)
+    nbc = [[cs.BC_NON_REFLECTIVE, cs.BC_PERIODIC, cs.BC_PERIODIC]] * 2 if xphys else None
+    s = make(dims, prec, refine=refine, nbc=nbc)
     out = torch.zeros(q.size, dtype=torch.float64, device="cuda")
     s.rhs(torch.from_numpy(q).cuda(), out)
     torch.cuda.synchronize()
