@@ -217,13 +217,22 @@ __device__ __forceinline__ void solve_fields_mx(float *sm, int w, int lane, cons
                                                 int nstart, int nend, const Coeffs &cf,
                                                 const ChunkFactors<LT> &U) {
     if (CF) {
+        // full groups of G fields, then the NF % G remaining fields as one
+        // smaller group (no solve of a padding field)
         constexpr int G = REF && LT >= 16 ? 1 : CSB_CF_SOLVE_GROUP;
+        constexpr int NFULL = NF / G * G, REM = NF - NFULL;
 #pragma unroll 1
-        for (int c = 0; c < NF; c += G) {
+        for (int c = 0; c < NFULL; c += G) {
             float *lines[G];
 #pragma unroll
-            for (int g = 0; g < G; ++g) lines[g] = field_line32<LT, TL>(sm, c + g < NF ? c + g : c, w);
-            solve_lines_cf<LT, G, REF>(lines, NF - c, lane, tab, U, cf);
+            for (int g = 0; g < G; ++g) lines[g] = field_line32<LT, TL>(sm, c + g, w);
+            solve_lines_cf<LT, G, REF>(lines, G, lane, tab, U, cf);
+        }
+        if constexpr (REM > 0) {
+            float *lines[REM];
+#pragma unroll
+            for (int g = 0; g < REM; ++g) lines[g] = field_line32<LT, TL>(sm, NFULL + g, w);
+            solve_lines_cf<LT, REM, REF>(lines, REM, lane, tab, U, cf);
         }
         return;
     }

@@ -32,6 +32,13 @@ namespace csb {
 
 constexpr int kErrTmaMxTimeout = 0x7102;
 
+// fields per warp solve of the ChunkFactors form without the sweep (all four
+// fields of a line in one solve: 256^3 gradient y / z passes 0.195 / 0.202 ->
+// 0.164 / 0.160 ms against two solves of two fields)
+#ifndef CSB_TMA_MX_GROUP
+#define CSB_TMA_MX_GROUP 4
+#endif
+
 template <int LT>
 constexpr int tma_mx_tile() {
     return LT <= 8 ? 8 : 4;
@@ -47,7 +54,7 @@ k_grad_mx_tma(const __grid_constant__ CUtensorMap smap, float *__restrict__ g, D
     constexpr int TL = tma_mx_tile<LT>();
     constexpr int NT = 256;
     constexpr int FPW = 4 * TL / (NT / 32);  // fields per warp: 4 (TL 8) or 2 (TL 4)
-    constexpr int G = (MODE == 1 || MODE == 3) && LT >= 16 ? 1 : 2;
+    constexpr int G = (MODE == 1 || MODE == 3) && LT >= 16 ? 1 : (MODE == 2 && FPW % CSB_TMA_MX_GROUP == 0 ? CSB_TMA_MX_GROUP : 2);
     using L = LineLayout<LT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int stage_elems = geo.nbox * 4 * TL * geo.boxlen;
