@@ -127,8 +127,11 @@ __device__ __forceinline__ void solve_line_mx(float *line, int lane, const DevTa
 #ifndef CSB_MX_SOLVE_GROUP
 #define CSB_MX_SOLVE_GROUP 2
 #endif
+// fields per warp solve of the ChunkFactors form (four: the flux passes solve
+// five fields as 4 + 1; measured against 2 + 2 + 1 at 256^3, flux z + RK
+// 0.720 -> 0.690 ms, the mixed step 7.47 -> 7.36 ms)
 #ifndef CSB_CF_SOLVE_GROUP
-#define CSB_CF_SOLVE_GROUP 2
+#define CSB_CF_SOLVE_GROUP 4
 #endif
 // resident 256-thread CTAs per SM asked of the compiler (register cap) for
 // the mixed one-phase flux passes with ChunkFactors and no refinement sweep
