@@ -253,7 +253,7 @@ k_grad_tma(const __grid_constant__ CUtensorMap qmap, double *__restrict__ g, Dev
 int tma_grad_map(int axis, const cs_dcomp &d, const TmaGeom &g, const double *q, CUtensorMap &map);
 // Tensor map over nf consecutive fields [nf][lmx] starting at base, boxes of
 // tl lines by boxlen points along `axis` by nf fields.
-int tma_field_map(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const double *base, CUtensorMap &map);
+// (tma_field_map / tma_field_map32: declared in fused_mixed.cuh)
 
 template <int LT, int AXIS>
 int launch_grad_tma_t(const PassArgs &a, const cs_dcomp &d, const double *q, bool dtred, int *err,

@@ -154,8 +154,6 @@ k_grad_mx_tma(const __grid_constant__ CUtensorMap smap, float *__restrict__ g, D
     }
 }
 
-// Host side (tma_grad.cu): tensor map over nf consecutive FP32 fields.
-int tma_field_map32(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const float *base, CUtensorMap &map);
 
 template <int LT, int AXIS>
 int launch_grad_mx_tma_t(const MixedArgs &a, const cs_dcomp &d, int *err, cudaStream_t st) {
