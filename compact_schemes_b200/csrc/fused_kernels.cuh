@@ -2,6 +2,8 @@
 // their launch templates (instantiated per axis in fused_axis{0,1,2}.cu).
 #pragma once
 
+#include <cuda.h>
+
 #include <cmath>
 
 #include "context.h"
@@ -40,6 +42,41 @@
 #endif
 
 namespace csb {
+
+// L2 prefetch of one box of a tensor map (cp.async.bulk.prefetch.tensor: a
+// hint with nothing to wait for; the map covers this GPU's memory only).
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap *map, int c0, int c1, int c2) {
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(c0), "r"(c1), "r"(c2)
+                 : "memory");
+}
+__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap *map, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+}
+
+// Geometry of the L2 prefetch of a flux pass's read-modify-write inputs: the
+// tile's lines of the RHS accumulator R and, in the RK modes, of q^n, as boxes
+// of TL lines by boxlen points along the line by five fields.
+struct FluxPrefetch {
+    int on;      // 0: no prefetch (the maps are not valid)
+    int nbox;    // boxes along the line (1 or 2)
+    int boxlen;  // points per box along the line
+    int lxi;     // points per x row (y tiles)
+};
+
+// Issue the prefetch boxes of the tile starting at line line0 (one thread).
+template <int AXIS>
+__device__ __forceinline__ void prefetch_tile(const CUtensorMap *map, const FluxPrefetch &pf, int64_t line0) {
+    for (int b = 0; b < pf.nbox; ++b) {
+        if (AXIS == 0) tma_prefetch_3d(map, b * pf.boxlen, (int)line0, 0);
+        else if (AXIS == 1) tma_prefetch_4d(map, (int)(line0 % pf.lxi), b * pf.boxlen, (int)(line0 / pf.lxi), 0);
+        else tma_prefetch_3d(map, (int)line0, b * pf.boxlen, 0);
+    }
+}
 
 struct Phys {
     double M[3][3];  // metric rows xim, etm, zem (J^-1 grad xi_a)
@@ -353,7 +390,9 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
                                           const double *__restrict__ qn, double *__restrict__ qout,
                                           double *__restrict__ drva, const DevTables<double> &tab, int lxi, int let,
                                           int64_t lmx, int64_t F, int nstart, int nend, const Coeffs &cf,
-                                          const Phys &ph, const RkParams &rk, const FieldMet &fm = FieldMet{}) {
+                                          const Phys &ph, const RkParams &rk, const FieldMet &fm = FieldMet{},
+                                          const CUtensorMap *pf_r = nullptr, const CUtensorMap *pf_q = nullptr,
+                                          const FluxPrefetch *pfg = nullptr) {
     using L = LineLayout<LT>;
     const int n = tab.n;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -365,6 +404,12 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
 #pragma unroll
         for (int m = 0; m < 5; ++m) field_line<LT, TL>(sm, m, l)[pj] = fl[m];
     });
+    // the RK store phase's R and q^n of this tile, fetched into L2 while the
+    // tile is solved
+    if (MODE >= kAccumRk && pfg && pfg->on && threadIdx.x == 0) {
+        if (MODE != kWriteRk) prefetch_tile<AXIS>(pf_r, *pfg, line0);
+        prefetch_tile<AXIS>(pf_q, *pfg, line0);
+    }
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
     if (fidx < F) {
@@ -427,12 +472,13 @@ __global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_FLUX_MINB : 1)
 k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__restrict__ rhs,
        const double *__restrict__ qn, double *__restrict__ qout, double *__restrict__ drva,
        DevTables<double> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend,
-       Coeffs cf, Phys ph, RkParams rk, FieldMet fm) {
+       Coeffs cf, Phys ph, RkParams rk, FieldMet fm, const __grid_constant__ CUtensorMap pf_r,
+       const __grid_constant__ CUtensorMap pf_q, FluxPrefetch pfg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK);
     flux_tile<LT, AXIS, TL, MODE, VISC, false, P, FM>(reinterpret_cast<double *>(smem_raw), (int64_t)blockIdx.x * TL,
                                                       q, g, rhs, qn, qout, drva, tab, lxi, let, lmx, F, nstart, nend,
-                                                      cf, ph, rk, fm);
+                                                      cf, ph, rk, fm, &pf_r, &pf_q, &pfg);
 }
 
 
@@ -478,6 +524,43 @@ inline int set_smem(KernelT kern, size_t bytes) {
     return CS_OK;
 }
 
+// Host side (tma_grad.cu): tensor maps over nf consecutive fields, boxes of
+// tl lines by boxlen points along `axis` by nf fields.
+int tma_field_map(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const double *base, CUtensorMap &map);
+int tma_field_map32(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const float *base, CUtensorMap &map);
+inline int tma_field_map_t(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const double *base,
+                           CUtensorMap &map) {
+    return tma_field_map(axis, d, tl, boxlen, nf, base, map);
+}
+inline int tma_field_map_t(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const float *base,
+                           CUtensorMap &map) {
+    return tma_field_map32(axis, d, tl, boxlen, nf, base, map);
+}
+
+// Prefetch geometry and tensor maps of a flux pass with the RK update (none
+// for the other modes; none where the rows or field blocks are not 16-byte
+// multiples, or the lines are longer than two boxes).  RT: element type of
+// the RHS accumulator R.
+template <int AXIS, int TL, int MODE, typename RT>
+FluxPrefetch flux_prefetch(const PassArgs &b, const RT *rhs, const double *qn, CUtensorMap &mr, CUtensorMap &mq) {
+    FluxPrefetch pf{};
+    if (MODE < kAccumRk) return pf;
+    const int lze = (int)(b.lmx / ((int64_t)b.lxi * b.let));
+    const cs_dcomp d{(int)b.lmx, b.lxi, b.let, lze};
+    const int n = AXIS == 0 ? b.lxi : (AXIS == 1 ? b.let : lze);
+    if (n > 512 || b.lmx % 4 || (AXIS < 2 ? b.lxi % 4 : ((int64_t)b.lxi * b.let) % 4)) return pf;
+    if (reinterpret_cast<uintptr_t>(rhs) % 16 || reinterpret_cast<uintptr_t>(qn) % 16) return pf;
+    pf.nbox = n > 256 ? 2 : 1;
+    // box starts along the line (the innermost coordinate for x lines) on
+    // 16-byte boundaries; boxes that reach past the line read nothing
+    pf.boxlen = ((n + pf.nbox - 1) / pf.nbox + 3) / 4 * 4;
+    pf.lxi = b.lxi;
+    if (MODE != kWriteRk && tma_field_map_t(AXIS, d, TL, pf.boxlen, 5, rhs, mr)) return FluxPrefetch{};
+    if (tma_field_map_t(AXIS, d, TL, pf.boxlen, 5, qn, mq)) return FluxPrefetch{};
+    pf.on = 1;
+    return pf;
+}
+
 template <int LT, int AXIS, int TL>
 int launch_grad_t(const PassArgs &a, const double *q, bool dtred, cudaStream_t st) {
     const size_t smem = (size_t)4 * TL * LineLayout<LT>::kSlot * sizeof(double);
@@ -499,8 +582,10 @@ int launch_flux_t(const PassArgs &a, const double *q, const double *qn, double *
     if (a.fm.xim) kern = a.viscous ? k_flux<LT, AXIS, TL, MODE, true, true> : k_flux<LT, AXIS, TL, MODE, false, true>;
     if (int rc = set_smem(kern, smem)) return rc;
     const unsigned blocks = (unsigned)((a.F + TL - 1) / TL);
+    CUtensorMap mr{}, mq{};
+    const FluxPrefetch pfg = flux_prefetch<AXIS, TL, MODE>(a, a.rhs, qn, mr, mq);
     kern<<<blocks, TL * 32, smem, st>>>(q, a.grad, a.rhs, qn, qout, drva, a.tab->t64, a.lxi, a.let, a.lmx,
-                                        a.F, a.nstart, a.nend, a.cf, a.ph, rk, a.fm);
+                                        a.F, a.nstart, a.nend, a.cf, a.ph, rk, a.fm, mr, mq, pfg);
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }

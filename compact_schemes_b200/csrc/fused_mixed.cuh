@@ -29,46 +29,6 @@
 
 namespace csb {
 
-// L2 prefetch of one box of a tensor map (cp.async.bulk.prefetch.tensor: a
-// hint with nothing to wait for; the map covers this GPU's memory only).
-__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap *map, int c0, int c1, int c2) {
-    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(c0), "r"(c1), "r"(c2)
-                 : "memory");
-}
-__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap *map, int c0, int c1, int c2, int c3) {
-    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(c0), "r"(c1), "r"(c2), "r"(c3)
-                 : "memory");
-}
-
-// Geometry of the L2 prefetch of a flux pass's read-modify-write inputs: the
-// tile's lines of the RHS accumulator R and, in the RK modes, of q^n, as boxes
-// of TL lines by boxlen points along the line by five fields.
-struct FluxPrefetch {
-    int on;      // 0: no prefetch (the maps are not valid)
-    int nbox;    // boxes along the line (1 or 2)
-    int boxlen;  // points per box along the line
-    int lxi;     // points per x row (y tiles)
-};
-
-// Issue the prefetch boxes of the tile starting at line line0 (one thread).
-template <int AXIS>
-__device__ __forceinline__ void prefetch_tile(const CUtensorMap *map, const FluxPrefetch &pf, int64_t line0) {
-    for (int b = 0; b < pf.nbox; ++b) {
-        if (AXIS == 0) tma_prefetch_3d(map, b * pf.boxlen, (int)line0, 0);
-        else if (AXIS == 1) tma_prefetch_4d(map, (int)(line0 % pf.lxi), b * pf.boxlen, (int)(line0 / pf.lxi), 0);
-        else tma_prefetch_3d(map, (int)line0, b * pf.boxlen, 0);
-    }
-}
-
-// Host side (tma_grad.cu): tensor maps over nf consecutive fields, boxes of
-// tl lines by boxlen points along `axis` by nf fields.
-int tma_field_map(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const double *base, CUtensorMap &map);
-int tma_field_map32(int axis, const cs_dcomp &d, int tl, int boxlen, int nf, const float *base, CUtensorMap &map);
-
 constexpr double kRho0 = 1.0;
 constexpr double kP0 = 1.0 / kGam;
 constexpr double kT0 = kGam * kP0 / kRho0;  // = 1
@@ -515,12 +475,6 @@ k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__re
     const int n = tab.n;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t line0 = (int64_t)blockIdx.x * TL;
-    // the store phase's R (and q^n) of this tile, fetched into L2 while the
-    // tile is loaded and solved
-    if (MODE != kWrite && pfg.on && threadIdx.x == 0) {
-        if (MODE != kWriteRk) prefetch_tile<AXIS>(&pf_r, pfg, line0);
-        if (MODE >= kAccumRk) prefetch_tile<AXIS>(&pf_q, pfg, line0);
-    }
     const PhysF pf = phys_f32(ph);
     tile_for_each<AXIS, TL, CSB_MX_FLUX_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         float fl[5];
@@ -530,6 +484,14 @@ k_flux_mx(const float *__restrict__ sh, const float *__restrict__ g, float *__re
 #pragma unroll
         for (int m = 0; m < 5; ++m) field_line32<LT, TL>(sm, m, l)[pj] = fl[m];
     });
+    // the RK store phase's R and q^n of this tile, fetched into L2 while the
+    // tile is solved (measured at 256^3: flux z + RK 0.689 -> 0.639 ms; issued
+    // before the load phase it competed with it and was slower, and the
+    // R-only prefetch of the accumulate pass did not pay)
+    if (MODE >= kAccumRk && pfg.on && threadIdx.x == 0) {
+        if (MODE != kWriteRk) prefetch_tile<AXIS>(&pf_r, pfg, line0);
+        prefetch_tile<AXIS>(&pf_q, pfg, line0);
+    }
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
     if (fidx < F) {
@@ -654,30 +616,6 @@ int launch_grad_mx_t(const MixedArgs &a, const double *q, bool first, cudaStream
                                         chunk_factors_of<LT>(*b.tab));
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
-}
-
-// Prefetch geometry and tensor maps of a flux pass (none for kWrite, which
-// reads no R; none where the rows or field blocks are not 16-byte multiples,
-// or the lines are longer than two boxes).
-template <int AXIS, int TL, int MODE>
-FluxPrefetch flux_prefetch(const PassArgs &b, const float *rhs, const double *qn, CUtensorMap &mr, CUtensorMap &mq) {
-    FluxPrefetch pf{};
-    if (MODE == kWrite) return pf;
-    const int lze = (int)(b.lmx / ((int64_t)b.lxi * b.let));
-    const cs_dcomp d{(int)b.lmx, b.lxi, b.let, lze};
-    const int n = AXIS == 0 ? b.lxi : (AXIS == 1 ? b.let : lze);
-    if (n > 512 || b.lmx % 4 || (AXIS < 2 ? b.lxi % 4 : ((int64_t)b.lxi * b.let) % 4)) return pf;
-    if (reinterpret_cast<uintptr_t>(rhs) % 16 || (MODE >= kAccumRk && reinterpret_cast<uintptr_t>(qn) % 16))
-        return pf;
-    pf.nbox = n > 256 ? 2 : 1;
-    // box starts along the line (the innermost coordinate for x lines) on
-    // 16-byte boundaries; boxes that reach past the line read nothing
-    pf.boxlen = ((n + pf.nbox - 1) / pf.nbox + 3) / 4 * 4;
-    pf.lxi = b.lxi;
-    if (MODE != kWriteRk && tma_field_map32(AXIS, d, TL, pf.boxlen, 5, rhs, mr)) return FluxPrefetch{};
-    if (MODE >= kAccumRk && tma_field_map(AXIS, d, TL, pf.boxlen, 5, qn, mq)) return FluxPrefetch{};
-    pf.on = 1;
-    return pf;
 }
 
 template <int LT, int AXIS, int TL, int MODE>
