@@ -390,9 +390,7 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
                                           const double *__restrict__ qn, double *__restrict__ qout,
                                           double *__restrict__ drva, const DevTables<double> &tab, int lxi, int let,
                                           int64_t lmx, int64_t F, int nstart, int nend, const Coeffs &cf,
-                                          const Phys &ph, const RkParams &rk, const FieldMet &fm = FieldMet{},
-                                          const CUtensorMap *pf_r = nullptr, const CUtensorMap *pf_q = nullptr,
-                                          const FluxPrefetch *pfg = nullptr) {
+                                          const Phys &ph, const RkParams &rk, const FieldMet &fm = FieldMet{}) {
     using L = LineLayout<LT>;
     const int n = tab.n;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -404,12 +402,6 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
 #pragma unroll
         for (int m = 0; m < 5; ++m) field_line<LT, TL>(sm, m, l)[pj] = fl[m];
     });
-    // the RK store phase's R and q^n of this tile, fetched into L2 while the
-    // tile is solved
-    if (MODE >= kAccumRk && pfg && pfg->on && threadIdx.x == 0) {
-        if (MODE != kWriteRk) prefetch_tile<AXIS>(pf_r, *pfg, line0);
-        prefetch_tile<AXIS>(pf_q, *pfg, line0);
-    }
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
     if (fidx < F) {
@@ -472,13 +464,12 @@ __global__ void __launch_bounds__(TL * 32, TL == 8 ? CSB_FLUX_MINB : 1)
 k_flux(const double *__restrict__ q, const double *__restrict__ g, double *__restrict__ rhs,
        const double *__restrict__ qn, double *__restrict__ qout, double *__restrict__ drva,
        DevTables<double> tab, int lxi, int let, int64_t lmx, int64_t F, int nstart, int nend,
-       Coeffs cf, Phys ph, RkParams rk, FieldMet fm, const __grid_constant__ CUtensorMap pf_r,
-       const __grid_constant__ CUtensorMap pf_q, FluxPrefetch pfg) {
+       Coeffs cf, Phys ph, RkParams rk, FieldMet fm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK);
     flux_tile<LT, AXIS, TL, MODE, VISC, false, P, FM>(reinterpret_cast<double *>(smem_raw), (int64_t)blockIdx.x * TL,
                                                       q, g, rhs, qn, qout, drva, tab, lxi, let, lmx, F, nstart, nend,
-                                                      cf, ph, rk, fm, &pf_r, &pf_q, &pfg);
+                                                      cf, ph, rk, fm);
 }
 
 
@@ -540,7 +531,9 @@ inline int tma_field_map_t(int axis, const cs_dcomp &d, int tl, int boxlen, int 
 // Prefetch geometry and tensor maps of a flux pass with the RK update (none
 // for the other modes; none where the rows or field blocks are not 16-byte
 // multiples, or the lines are longer than two boxes).  RT: element type of
-// the RHS accumulator R.
+// the RHS accumulator R.  The mixed form's RK pass uses it; in the FP64 RK
+// pass, whose R and q^n are 80 B/pt, it measured slower at 256^3
+// (flux z + RK 0.849 -> 0.891 ms) and is not used.
 template <int AXIS, int TL, int MODE, typename RT>
 FluxPrefetch flux_prefetch(const PassArgs &b, const RT *rhs, const double *qn, CUtensorMap &mr, CUtensorMap &mq) {
     FluxPrefetch pf{};
@@ -582,10 +575,8 @@ int launch_flux_t(const PassArgs &a, const double *q, const double *qn, double *
     if (a.fm.xim) kern = a.viscous ? k_flux<LT, AXIS, TL, MODE, true, true> : k_flux<LT, AXIS, TL, MODE, false, true>;
     if (int rc = set_smem(kern, smem)) return rc;
     const unsigned blocks = (unsigned)((a.F + TL - 1) / TL);
-    CUtensorMap mr{}, mq{};
-    const FluxPrefetch pfg = flux_prefetch<AXIS, TL, MODE>(a, a.rhs, qn, mr, mq);
     kern<<<blocks, TL * 32, smem, st>>>(q, a.grad, a.rhs, qn, qout, drva, a.tab->t64, a.lxi, a.let, a.lmx,
-                                        a.F, a.nstart, a.nend, a.cf, a.ph, rk, a.fm, mr, mq, pfg);
+                                        a.F, a.nstart, a.nend, a.cf, a.ph, rk, a.fm);
     CSB_CUDA(cudaGetLastError());
     return CS_OK;
 }
