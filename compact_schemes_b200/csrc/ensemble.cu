@@ -362,13 +362,13 @@ int cs_ensemble_autotune(cs_ensemble *e, const double *q, int reps, cs_ensemble_
     for (int w : {8, 4, 2, 1})
         if (w < e->nbox) windows.push_back(w);
     std::vector<int> tiles = e->lt_max > 4 ? std::vector<int>{4} : std::vector<int>{8, 4};
-    const int chunks[] = {2, 4, 8};
+    const int chunks[] = {2, 4, 8, 16};
     const cs_ensemble_tuning saved = e->tune;
     cs_ensemble_tuning win = saved;
     double win_ms = 1e300;
     int rc = CS_OK;
     for (int tile : tiles) {
-        for (int ci = 0; ci < 3 && !rc; ++ci)
+        for (int ci = 0; ci < 4 && !rc; ++ci)
         for (int w : windows) {
             cs_ensemble_tuning t{w, tile, 0, chunks[ci]};
             if ((rc = cs_ensemble_set_tuning(e, &t))) break;

@@ -89,6 +89,22 @@ static __constant__ Coeffs c_ens_cf;
 // the per-box passes: the items have fewer registers to spare).
 constexpr int kEnsRmwChunk = 2, kEnsRmwChunkRk = 1;
 
+// Line solves of the work items: fields per warp solve for lines of up to 128
+// points (LT <= 4), and whether the periodic closure rows are formed
+// lane-parallel (8 lanes per field line) instead of by the two owner lanes.
+// Short lines make the serial closure sums a large share of the solve, which
+// runs on one lane while the other 31 wait.
+#ifndef CSB_ENS_SG
+#define CSB_ENS_SG 4
+#endif
+#ifndef CSB_ENS_ROWS
+#define CSB_ENS_ROWS 1
+#endif
+template <int LT>
+constexpr int ens_solve_group() {
+    return LT <= 4 ? CSB_ENS_SG : 2;
+}
+
 // One work item of pass KIND for chunk length LT, inlined into the stage
 // kernel (with the box parameters in constant memory the combined body spills
 // little; separate functions measured slower by their call overhead).
@@ -102,12 +118,15 @@ __device__ __forceinline__ void ens_item(const EnsArgs &a, int b, int64_t line0,
     const Phys &ph = bx.ph;
     const DevTables<double> &tab = bx.tab[AX];
     if (KIND < 3) {
+        constexpr int SG = ens_solve_group<LT>();
+        constexpr bool ROWS = CSB_ENS_ROWS != 0;
         if (KIND == 0 && stage == 0)
-            grad_tile<LT, 0, TL, true>(sm, line0, qin, g, tab, bx.lxi, bx.let, bx.lmx, bx.F[0], bx.nstart[0],
-                                       bx.nend[0], c_ens_cf, ph, a.dtacc + 2 * b);
+            grad_tile<LT, 0, TL, true, false, SG, ROWS>(sm, line0, qin, g, tab, bx.lxi, bx.let, bx.lmx, bx.F[0],
+                                                        bx.nstart[0], bx.nend[0], c_ens_cf, ph, a.dtacc + 2 * b);
         else
-            grad_tile<LT, AX, TL, false>(sm, line0, qin, g + 4 * AX * bx.lmx, tab, bx.lxi, bx.let, bx.lmx,
-                                         bx.F[AX], bx.nstart[AX], bx.nend[AX], c_ens_cf, ph, nullptr);
+            grad_tile<LT, AX, TL, false, false, SG, ROWS>(sm, line0, qin, g + 4 * AX * bx.lmx, tab, bx.lxi, bx.let,
+                                                          bx.lmx, bx.F[AX], bx.nstart[AX], bx.nend[AX], c_ens_cf, ph,
+                                                          nullptr);
         return;
     }
     double *rhs = a.rhs + bx.roff;
@@ -123,8 +142,9 @@ __device__ __forceinline__ void ens_item(const EnsArgs &a, int b, int64_t line0,
     double *qout = (stage == 3 ? a.q : a.q1) + bx.qoff;
     constexpr int MODE = KIND == 3 ? kWrite : (KIND == 4 ? kAccum : kAccumRk);
     constexpr int P = MODE == kAccum ? kEnsRmwChunk : kEnsRmwChunkRk;
-    flux_tile<LT, AX, TL, MODE, VISC, true, P>(sm, line0, qin, g, rhs, qn, qout, nullptr, tab, bx.lxi, bx.let,
-                                               bx.lmx, bx.F[AX], bx.nstart[AX], bx.nend[AX], c_ens_cf, ph, rk);
+    flux_tile<LT, AX, TL, MODE, VISC, true, P, false, ens_solve_group<LT>(), CSB_ENS_ROWS != 0>(
+        sm, line0, qin, g, rhs, qn, qout, nullptr, tab, bx.lxi, bx.let, bx.lmx, bx.F[AX], bx.nstart[AX], bx.nend[AX],
+        c_ens_cf, ph, rk);
 }
 
 template <int TL, bool VISC, int LT>

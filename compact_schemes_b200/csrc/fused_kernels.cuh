@@ -161,52 +161,63 @@ __device__ __forceinline__ double *field_line(double *sm, int field, int line) {
     return sm + (field * TL + line) * LineLayout<LT>::kSlot;
 }
 
-// Solve the derivative of NF fields of this warp's line held in shared memory
-// and overwrite them with the result; G fields share one warp_solve call
+// Solve fields c0 .. c0+G-1 (those below NF) of this warp's line held in
+// shared memory and overwrite them with the result, in one warp_solve call
 // (their table loads and shuffles are interleaved).  ROWS: the single-rank
-// periodic closure rows of a group are formed on 8 lanes per line
+// periodic closure rows of the group are formed on 8 lanes per line
 // (group_closure_rows) instead of serially by the owner lanes; bit-identical
-// either way, and faster only where registers allow it (measured: the
-// one-phase FP64 passes keep the serial form).
-template <int LT, int TL, int NF, int G = CSB_SOLVE_GROUP, bool ROWS = false>
-__device__ __forceinline__ void solve_fields(double *sm, int w, int lane, const DevTables<double> &tab,
-                                             int nstart, int nend, const Coeffs &cf) {
-#pragma unroll 1
-    for (int c0 = 0; c0 < NF; c0 += G) {
-        double d[G][LT];
-        // single-rank periodic closures: the group's closure sums on 8 lanes per line
-        double *lines[G];
+// either way.
+template <int LT, int TL, int NF, int G, bool ROWS>
+__device__ __forceinline__ void solve_field_group(double *sm, int w, int lane, const DevTables<double> &tab,
+                                                  int nstart, int nend, const Coeffs &cf, int c0) {
+    double d[G][LT];
+    double *lines[G];
 #pragma unroll
-        for (int g = 0; g < G; ++g) lines[g] = field_line<LT, TL>(sm, c0 + g < NF ? c0 + g : c0, w);
-        const bool sums = ROWS && (nstart != 0 || nend != 0);
-        const double rows = sums ? group_closure_rows<LT, double, double, G>(lines, NF - c0, tab.n, lane, cf) : 0.0;
+    for (int g = 0; g < G; ++g) lines[g] = field_line<LT, TL>(sm, c0 + g < NF ? c0 + g : c0, w);
+    const bool sums = ROWS && (nstart != 0 || nend != 0);
+    const double rows = sums ? group_closure_rows<LT, double, double, G>(lines, NF - c0, tab.n, lane, cf) : 0.0;
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-            double own2[2];
-            if (sums) take_closure_rows(rows, g, lane, own2);
-            if (c0 + g < NF) deriv_rhs<LT, double, double>(lines[g], tab.n, lane, nstart, nend, nullptr, cf, d[g],
-                                                           sums ? own2 : nullptr);
-            else {
+    for (int g = 0; g < G; ++g) {
+        double own2[2];
+        if (sums) take_closure_rows(rows, g, lane, own2);
+        if (c0 + g < NF) deriv_rhs<LT, double, double>(lines[g], tab.n, lane, nstart, nend, nullptr, cf, d[g],
+                                                       sums ? own2 : nullptr);
+        else {
 #pragma unroll
-                for (int t = 0; t < LT; ++t) d[g][t] = 0.0;
-            }
+            for (int t = 0; t < LT; ++t) d[g][t] = 0.0;
         }
-        warp_solve<LT, G, double>(tab, d, lane);
-        __syncwarp();
+    }
+    warp_solve<LT, G, double>(tab, d, lane);
+    __syncwarp();
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-            if (c0 + g >= NF) continue;
-            double *line = field_line<LT, TL>(sm, c0 + g, w);
+    for (int g = 0; g < G; ++g) {
+        if (c0 + g >= NF) continue;
+        double *line = field_line<LT, TL>(sm, c0 + g, w);
 #pragma unroll
-            for (int t = 0; t < LT; ++t)
-                if (lane * LT + t < tab.n) line[LineLayout<LT>::pos_ct(lane, t)] = d[g][t];
-        }
+        for (int t = 0; t < LT; ++t)
+            if (lane * LT + t < tab.n) line[LineLayout<LT>::pos_ct(lane, t)] = d[g][t];
     }
 }
 
+// Solve the derivative of NF fields of this warp's line, G fields per
+// warp_solve call (solve_field_group).  With ROWS a last group of fewer than
+// G fields is solved as a group of its own size; without, it is padded with
+// zero right-hand sides (measured: the one-phase FP64 passes keep the serial
+// closure form and the padded group).
+template <int LT, int TL, int NF, int G = CSB_SOLVE_GROUP, bool ROWS = false>
+__device__ __forceinline__ void solve_fields(double *sm, int w, int lane, const DevTables<double> &tab,
+                                             int nstart, int nend, const Coeffs &cf) {
+    constexpr int REM = ROWS ? NF % G : 0;
+    constexpr int NFULL = NF - REM;
+#pragma unroll 1
+    for (int c0 = 0; c0 < NFULL; c0 += G) solve_field_group<LT, TL, NF, G, ROWS>(sm, w, lane, tab, nstart, nend, cf, c0);
+    if constexpr (REM > 0) solve_field_group<LT, TL, NF, REM, ROWS>(sm, w, lane, tab, nstart, nend, cf, NFULL);
+}
+
 // One tile of the gradient pass: lines line0 .. line0+TL-1 (TL * 32 threads;
-// sm holds 4 * TL line slots).
-template <int LT, int AXIS, int TL, bool DTRED, bool FM = false>
+// sm holds 4 * TL line slots).  SG: fields per warp solve (0: the pass
+// default); ROWS: periodic closure rows formed lane-parallel (solve_fields).
+template <int LT, int AXIS, int TL, bool DTRED, bool FM = false, int SG = 0, bool ROWS = false>
 __device__ __forceinline__ void grad_tile(double *sm, int64_t line0, const double *__restrict__ q,
                                           double *__restrict__ g, const DevTables<double> &tab, int lxi, int let,
                                           int64_t lmx, int64_t F, int nstart, int nend, const Coeffs &cf,
@@ -249,7 +260,9 @@ __device__ __forceinline__ void grad_tile(double *sm, int64_t line0, const doubl
     });
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
-    if (fidx < F) solve_fields<LT, TL, 4, (LT >= 16 ? 1 : CSB_GRAD_SOLVE_GROUP)>(sm, w, lane, tab, nstart, nend, cf);
+    if (fidx < F)
+        solve_fields<LT, TL, 4, (SG > 0 ? SG : (LT >= 16 ? 1 : CSB_GRAD_SOLVE_GROUP)), ROWS>(sm, w, lane, tab, nstart,
+                                                                                         nend, cf);
     tile_sync<AXIS, TL>();
     tile_for_each<AXIS, TL, CSB_STORE_UNROLL>(line0, F, n, lxi, let, [&](int l, int j, int64_t gi) {
         const int pj = L::pos(j);
@@ -381,10 +394,10 @@ __device__ __forceinline__ void point_flux(const double *__restrict__ q, const d
 
 // One tile of the flux pass (TL * 32 threads; sm holds 5 * TL line slots).
 // CG: the RHS accumulator, gradients and CFL maxima come from other CTAs of
-// the same launch (ensemble) and are read from L2.
+// the same launch (ensemble) and are read from L2.  SG, ROWS: as grad_tile.
 template <int LT, int AXIS, int TL, int MODE, bool VISC, bool CG = false,
           int P = MODE == kAccum ? (LT >= 16 ? 2 : CSB_RMW_CHUNK) : (LT >= 16 ? 1 : CSB_RMW_CHUNK_RK),
-          bool FM = false>
+          bool FM = false, int SG = 0, bool ROWS = false>
 __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const double *__restrict__ q,
                                           const double *__restrict__ g, double *__restrict__ rhs,
                                           const double *__restrict__ qn, double *__restrict__ qout,
@@ -405,7 +418,8 @@ __device__ __forceinline__ void flux_tile(double *sm, int64_t line0, const doubl
     tile_sync<AXIS, TL>();
     const int64_t fidx = line0 + w;
     if (fidx < F) {
-        solve_fields<LT, TL, 5, (LT >= 16 ? 1 : CSB_SOLVE_GROUP)>(sm, w, lane, tab, nstart, nend, cf);
+        solve_fields<LT, TL, 5, (SG > 0 ? SG : (LT >= 16 ? 1 : CSB_SOLVE_GROUP)), ROWS>(sm, w, lane, tab, nstart, nend,
+                                                                                    cf);
         if (drva) {
             // line-end derivatives for the characteristic boundary closure
             // (drva of deriv_kernel_2d, src/cuda/kernels/numerics_pc.hpp:237-248)

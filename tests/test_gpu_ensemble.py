@@ -55,7 +55,8 @@ def test_ensemble_matches_per_box_solvers(cuda, viscous):
 
 
 @pytest.mark.parametrize("tuning", [dict(window=0, tile=8, chunk=1), dict(window=2, tile=8, chunk=16),
-                                    dict(window=1, tile=4, chunk=3), dict(window=3, tile=4, ctas_per_sm=1)])
+                                    dict(window=1, tile=4, chunk=3), dict(window=3, tile=4, ctas_per_sm=1),
+                                    dict(window=0, tile=8, chunk=16)])
 def test_ensemble_tunings_bit_identical(cuda, tuning):
     import torch
     import compact_schemes_b200 as cs
