@@ -38,14 +38,15 @@ struct DeviceTables {
 };
 
 // key: n, scheme, nstart, nend, alpha_f bits
-using TableKey = std::tuple<int, int, int, int, uint64_t>;
+using TableKey = std::tuple<int, int, int, int, uint64_t, int>;
 
 // Cache of device tables (one per device/line configuration).
 class TableCache {
 public:
     ~TableCache();
-    // Returns nullptr and sets the error on failure.
-    const DeviceTables *get(int n, int scheme, int nstart, int nend, double alpha_f);
+    // Returns nullptr and sets the error on failure.  min_lt: shortest chunk
+    // of the tables (build_tables).
+    const DeviceTables *get(int n, int scheme, int nstart, int nend, double alpha_f, int min_lt = 2);
 
 private:
     std::mutex mu_;

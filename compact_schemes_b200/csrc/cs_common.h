@@ -67,11 +67,13 @@ struct HostTables {
 };
 
 // Choose the per-lane chunk length (power of two) for a line of n points.
-int chunk_length(int n);
+int chunk_length(int n, int min_lt = 2);
 // Build tables for the tridiagonal matrix rows a (sub), b (diag), c (super)
 // of a line of n points.  cyclic: a[0] couples x[n-1] and c[n-1] couples x[0].
+// min_lt: shortest chunk (a power of two >= 2); the chunk doubles from there
+// until the line fits 32 lanes.
 bool build_tables(int n, const double *a, const double *b, const double *c, bool cyclic,
-                  HostTables &out);
+                  HostTables &out, int min_lt = 2);
 // Matrix rows of the compact derivative (build_system,
 // src/cuda/kernels/numerics_device_pc.hpp:176-293) for face flags nstart/nend.
 void deriv_rows(int n, int nstart, int nend, double *a, double *b, double *c);

@@ -228,7 +228,10 @@ int cs_ensemble_create(cs_ensemble **out, int nbox, const cs_solver_config *boxe
             const int s0 = bc_ndf(c.nbc[0][a]), s1 = bc_ndf(c.nbc[1][a]);
             if (s0 < 0 || s1 < 0) return fail(CS_ERR_INVALID, "boundary code");
             if (s0 != s1) return fail(CS_ERR_UNSUPPORTED, "both faces of an axis periodic or both physical");
-            const DeviceTables *t = e->tables.get(n[a], kDeriv, s0, s1, 0.0);
+            // lines of up to 64 points in chunks of 4 (at most 16 lanes): the
+            // work items then solve two fields per half-warp (fewer PCR steps
+            // per field than 2-point chunks over 32 lanes)
+            const DeviceTables *t = e->tables.get(n[a], kDeriv, s0, s1, 0.0, n[a] <= 64 ? 4 : 2);
             if (!t) { cs_ensemble_destroy(e); return CS_ERR_UNSUPPORTED; }
             bx.tab[a] = t->t64;
             bx.lt[a] = t->lt;

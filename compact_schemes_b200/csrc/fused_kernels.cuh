@@ -169,7 +169,64 @@ __device__ __forceinline__ double *field_line(double *sm, int field, int line) {
 // either way.
 template <int LT, int TL, int NF, int G, bool ROWS>
 __device__ __forceinline__ void solve_field_group(double *sm, int w, int lane, const DevTables<double> &tab,
+                                                  int nstart, int nend, const Coeffs &cf, int c0);
+
+// solve_field_group for an even G on a line of at most 16 chunks whose solve
+// needs at most 5 PCR steps: each half-warp solves G/2 of the fields (lanes
+// 16 s + c hold chunk c of fields c0 + s G/2 + g), so every shuffle and table
+// factor of the solve serves two fields at once.  The closure rows are formed
+// as in solve_field_group (8 lanes per field line) and the arithmetic of each
+// row is the same: bit-identical to it.
+template <int LT, int TL, int NF, int G>
+__device__ __forceinline__ void solve_field_group_halves(double *sm, int w, int lane, const DevTables<double> &tab,
+                                                         int nstart, int nend, const Coeffs &cf, int c0) {
+    constexpr int H = G / 2;
+    const int s = lane >> 4, c = lane & 15;
+    double *lines[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) lines[g] = field_line<LT, TL>(sm, c0 + g < NF ? c0 + g : c0, w);
+    const bool sums = nstart != 0 || nend != 0;
+    const double rows = sums ? group_closure_rows<LT, double, double, G>(lines, NF - c0, tab.n, lane, cf) : 0.0;
+    double d[H][LT];
+#pragma unroll
+    for (int g = 0; g < H; ++g) {
+        const int gg = s * H + g;
+        double own2[2];
+        if (sums) {
+            const int src = 8 * gg + (c == 0 ? 0 : 4);
+            own2[0] = __shfl_sync(0xffffffffu, rows, src);
+            own2[1] = __shfl_sync(0xffffffffu, rows, src + 1);
+        }
+        const double *line = field_line<LT, TL>(sm, c0 + gg < NF ? c0 + gg : c0, w);
+        if (c0 + gg < NF) deriv_rhs<LT, double, double>(line, tab.n, c, nstart, nend, nullptr, cf, d[g],
+                                                        sums ? own2 : nullptr);
+        else {
+#pragma unroll
+            for (int t = 0; t < LT; ++t) d[g][t] = 0.0;
+        }
+    }
+    warp_solve<LT, H, double, 16>(tab, d, c);
+    __syncwarp();
+#pragma unroll
+    for (int g = 0; g < H; ++g) {
+        const int gg = s * H + g;
+        if (c0 + gg >= NF) continue;
+        double *line = field_line<LT, TL>(sm, c0 + gg, w);
+#pragma unroll
+        for (int t = 0; t < LT; ++t)
+            if (c * LT + t < tab.n) line[LineLayout<LT>::pos_ct(c, t)] = d[g][t];
+    }
+}
+
+template <int LT, int TL, int NF, int G, bool ROWS>
+__device__ __forceinline__ void solve_field_group(double *sm, int w, int lane, const DevTables<double> &tab,
                                                   int nstart, int nend, const Coeffs &cf, int c0) {
+    if constexpr (ROWS && G % 2 == 0) {
+        if (tab.p <= 16 && tab.pcr <= 5) {
+            solve_field_group_halves<LT, TL, NF, G>(sm, w, lane, tab, nstart, nend, cf, c0);
+            return;
+        }
+    }
     double d[G][LT];
     double *lines[G];
 #pragma unroll

@@ -107,15 +107,17 @@ __host__ __device__ constexpr InteriorChunk<LT> interior_chunk() {
     return k;
 }
 
-template <int LT, int NV, typename CT>
+template <int LT, int NV, typename CT, int W = 32>
 __device__ __forceinline__ void warp_solve_interior(const DevTables<CT> &T, CT (&d)[NV][LT], int lane);
 
 // Solve NV right-hand sides held as d[v][t] by the lanes of one warp; the
-// solution overwrites d.  All 32 lanes must call it (warp shuffles).
-template <int LT, int NV, typename CT>
+// solution overwrites d.  All 32 lanes must call it (warp shuffles).  W < 32:
+// every W lanes solve a line of their own (lines with p <= W chunks and at
+// most log2(W) + 1 PCR steps), `lane` is the lane within its W-lane segment.
+template <int LT, int NV, typename CT, int W = 32>
 __device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][LT], int lane) {
     if (LT >= 2 && T.interior) {
-        warp_solve_interior<LT, NV, CT>(T, d, lane);
+        warp_solve_interior<LT, NV, CT, W>(T, d, lane);
         return;
     }
     const int len = lane_len(lane, LT, T.p, T.last_len);
@@ -150,8 +152,8 @@ __device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][L
         const CT ka = T.k1[lane], kb = T.k2[lane], kc = T.k1[32 + lane], kd = T.k2[32 + lane];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const CT up1 = __shfl_up_sync(0xffffffffu, y1[v], 1);
-            const CT dn0 = __shfl_down_sync(0xffffffffu, y0[v], 1);
+            const CT up1 = __shfl_up_sync(0xffffffffu, y1[v], 1, W);
+            const CT dn0 = __shfl_down_sync(0xffffffffu, y0[v], 1, W);
             const CT n0 = y0[v] - ka * up1 - kb * y1[v];
             const CT n1 = y1[v] - kc * y0[v] - kd * dn0;
             y0[v] = n0;
@@ -166,10 +168,10 @@ __device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][L
         const CT kc = T.k1[s * 64 + 32 + lane], kd = T.k2[s * 64 + 32 + lane];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const CT u0 = __shfl_up_sync(0xffffffffu, y0[v], dl);
-            const CT d0 = __shfl_down_sync(0xffffffffu, y0[v], dl);
-            const CT u1 = __shfl_up_sync(0xffffffffu, y1[v], dl);
-            const CT d1 = __shfl_down_sync(0xffffffffu, y1[v], dl);
+            const CT u0 = __shfl_up_sync(0xffffffffu, y0[v], dl, W);
+            const CT d0 = __shfl_down_sync(0xffffffffu, y0[v], dl, W);
+            const CT u1 = __shfl_up_sync(0xffffffffu, y1[v], dl, W);
+            const CT d1 = __shfl_down_sync(0xffffffffu, y1[v], dl, W);
             y0[v] = y0[v] - ka * u0 - kb * d0;
             y1[v] = y1[v] - kc * u1 - kd * d1;
         }
@@ -187,8 +189,8 @@ __device__ __forceinline__ void warp_solve(const DevTables<CT> &T, CT (&d)[NV][L
         }
         if (T.cyclic) {
             const CT last = len >= 2 ? X1 : X0;
-            const CT ya = __shfl_sync(0xffffffffu, X0, 0);
-            const CT yb = __shfl_sync(0xffffffffu, last, T.p - 1);
+            const CT ya = __shfl_sync(0xffffffffu, X0, 0, W);
+            const CT yb = __shfl_sync(0xffffffffu, last, T.p - 1, W);
             const CT beta = (ya + T.cyc_s2 * yb) * T.cyc_s1;
 #pragma unroll
             for (int t = 0; t < LT; ++t) d[v][t] -= beta * T.cycz[t * 32 + lane];
@@ -217,7 +219,7 @@ __device__ __forceinline__ double cf_fma(double a, double b, double c) { return 
 // structure of the tables fixes fwd2 = 0 for rows 0 and 1 of a chunk, bwd1 = 1
 // and bwd2 = 0 for row LT - 2, and bwd1 = 1 for rows 1 .. LT - 3; those
 // products are left out.  All 32 lanes must call it.
-template <int LT, int NV, typename CT>
+template <int LT, int NV, typename CT, int W = 32>
 __device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT, CT> &U, const DevTables<CT> &T,
                                               CT (&d)[NV][LT], int lane) {
     static_assert(LT >= 2, "chunk");
@@ -241,8 +243,8 @@ __device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT, CT> &U, con
         const CT ka = T.k1[lane], kb = T.k2[lane], kc = T.k1[32 + lane], kd = T.k2[32 + lane];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const CT up1 = __shfl_up_sync(0xffffffffu, y1[v], 1);
-            const CT dn0 = __shfl_down_sync(0xffffffffu, y0[v], 1);
+            const CT up1 = __shfl_up_sync(0xffffffffu, y1[v], 1, W);
+            const CT dn0 = __shfl_down_sync(0xffffffffu, y0[v], 1, W);
             const CT n0 = y0[v] - ka * up1 - kb * y1[v];
             const CT n1 = y1[v] - kc * y0[v] - kd * dn0;
             y0[v] = n0;
@@ -257,10 +259,10 @@ __device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT, CT> &U, con
         const CT kc = T.k1[s * 64 + 32 + lane], kd = T.k2[s * 64 + 32 + lane];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const CT u0 = __shfl_up_sync(0xffffffffu, y0[v], dl);
-            const CT d0 = __shfl_down_sync(0xffffffffu, y0[v], dl);
-            const CT u1 = __shfl_up_sync(0xffffffffu, y1[v], dl);
-            const CT d1 = __shfl_down_sync(0xffffffffu, y1[v], dl);
+            const CT u0 = __shfl_up_sync(0xffffffffu, y0[v], dl, W);
+            const CT d0 = __shfl_down_sync(0xffffffffu, y0[v], dl, W);
+            const CT u1 = __shfl_up_sync(0xffffffffu, y1[v], dl, W);
+            const CT d1 = __shfl_down_sync(0xffffffffu, y1[v], dl, W);
             y0[v] = y0[v] - ka * u0 - kb * d0;
             y1[v] = y1[v] - kc * u1 - kd * d1;
         }
@@ -278,7 +280,7 @@ __device__ __forceinline__ void warp_solve_cf(const ChunkFactors<LT, CT> &U, con
 
 // warp_solve for tables flagged `interior`: the per-row factors are the
 // compile-time interior_chunk<LT> values.
-template <int LT, int NV, typename CT>
+template <int LT, int NV, typename CT, int W>
 __device__ __forceinline__ void warp_solve_interior(const DevTables<CT> &T, CT (&d)[NV][LT], int lane) {
     if constexpr (LT >= 2) {
         constexpr InteriorChunk<LT> K = interior_chunk<LT>();
@@ -292,7 +294,7 @@ __device__ __forceinline__ void warp_solve_interior(const DevTables<CT> &T, CT (
             U.nra[t] = (CT)(-K.rca[t]);
             U.nrc[t] = (CT)(-K.rcc[t]);
         }
-        warp_solve_cf<LT, NV, CT>(U, T, d, lane);
+        warp_solve_cf<LT, NV, CT, W>(U, T, d, lane);
     }
 }
 

@@ -120,7 +120,7 @@ static void chunk_factors(const HostTables &h, bool &uniform, float *cfu) {
         }
 }
 
-static bool host_tables_for(int n, int scheme, int nstart, int nend, double af, HostTables &h) {
+static bool host_tables_for(int n, int scheme, int nstart, int nend, double af, HostTables &h, int min_lt = 2) {
     std::vector<double> a(n), b(n), c(n);
     bool cyclic = false;
     if (scheme == kDeriv) {
@@ -143,18 +143,18 @@ static bool host_tables_for(int n, int scheme, int nstart, int nend, double af, 
             }
         }
     }
-    return build_tables(n, a.data(), b.data(), c.data(), cyclic, h);
+    return build_tables(n, a.data(), b.data(), c.data(), cyclic, h, min_lt);
 }
 
-const DeviceTables *TableCache::get(int n, int scheme, int nstart, int nend, double af) {
+const DeviceTables *TableCache::get(int n, int scheme, int nstart, int nend, double af, int min_lt) {
     uint64_t bits = 0;
     if (scheme == kFilter || scheme == kFilterT) std::memcpy(&bits, &af, sizeof bits);
-    TableKey key{n, scheme, nstart ? 1 : 0, nend ? 1 : 0, bits};
+    TableKey key{n, scheme, nstart ? 1 : 0, nend ? 1 : 0, bits, min_lt};
     std::lock_guard<std::mutex> lk(mu_);
     auto it = map_.find(key);
     if (it != map_.end()) return it->second;
     auto *dt = new DeviceTables();
-    if (!host_tables_for(n, scheme, nstart, nend, af, dt->host)) {
+    if (!host_tables_for(n, scheme, nstart, nend, af, dt->host, min_lt)) {
         delete dt;
         set_error(CS_ERR_UNSUPPORTED, "line length %d outside [5, %d]", n, kMaxLine);
         return nullptr;

@@ -100,8 +100,8 @@ void compute_interface_coeffs(Coeffs &cf) {
 #define CSB_MIN_CHUNK 2
 #endif
 
-int chunk_length(int n) {
-    int lt = CSB_MIN_CHUNK;
+int chunk_length(int n, int min_lt) {
+    int lt = min_lt > CSB_MIN_CHUNK ? min_lt : CSB_MIN_CHUNK;
     while (lt < 32 && (n + lt - 1) / lt > 32) lt *= 2;
     return lt;
 }
@@ -143,7 +143,7 @@ static void thomas(int n, const double *a, const double *b, const double *c, con
 }
 
 bool build_tables(int n, const double *a_in, const double *b_in, const double *c_in, bool cyclic,
-                  HostTables &T) {
+                  HostTables &T, int min_lt) {
     if (n < 5 || n > kMaxLine) return false;
     std::vector<double> a(a_in, a_in + n), b(b_in, b_in + n), c(c_in, c_in + n);
     T = HostTables();
@@ -165,7 +165,7 @@ bool build_tables(int n, const double *a_in, const double *b_in, const double *c
         T.cyc_s1 = 1.0 / (1.0 + z[0] + T.cyc_s2 * z[n - 1]);
         T.cycz = z;  // reshaped below
     }
-    const int lt = chunk_length(n);
+    const int lt = chunk_length(n, min_lt);
     const int p = (n + lt - 1) / lt;
     T.lt = lt;
     T.p = p;

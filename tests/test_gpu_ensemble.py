@@ -1,6 +1,9 @@
-"""Batched ensemble on the GPU: every box bit-identical to its own per-box
-solver (which the solver tests pin to the FP64 oracle), for every tuning,
-plus one box against the oracle directly."""
+"""Batched ensemble on the GPU: every box against its own per-box solver
+(which the solver tests pin to the FP64 oracle) -- bit-identical where every
+axis has more than 64 points, within rounding where an axis has 64 or fewer
+(the ensemble solves those lines in 4-point chunks, the per-box solver in
+2-point chunks) -- every tuning bit-identical to the default tuning, plus one
+box against the oracle directly."""
 import numpy as np
 import pytest
 
@@ -9,7 +12,25 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 BOXES = [((32, 48, 40), 0.1, 1600.0), ((64, 32, 32), 0.25, 500.0), ((48, 48, 48), 0.05, 3000.0),
-         ((96, 32, 40), 0.2, 800.0), ((40, 128, 24), 0.15, 1200.0)]
+         ((96, 32, 40), 0.2, 800.0), ((40, 128, 24), 0.15, 1200.0), ((96, 72, 80), 0.12, 1000.0)]
+TOL = 1e-12  # per field; momenta relative to the largest momentum component
+
+
+def _rel_errs(got, ref):
+    g, r = got.view(5, -1), ref.view(5, -1)
+    mom = max(r[m].abs().max().item() for m in (1, 2, 3))
+    return [((g[m] - r[m]).abs().max().item() / (mom if m in (1, 2, 3) else r[m].abs().max().item()))
+            for m in range(5)]
+
+
+def _agrees(got, ref, dims):
+    """Bit-identical when every axis has more than 64 points, else within TOL."""
+    if min(dims) > 64:
+        assert bool((got == ref).all()), (dims, _rel_errs(got, ref))
+        return True
+    errs = _rel_errs(got, ref)
+    assert max(errs) < TOL, (dims, errs)
+    return True
 
 
 def _state(ens, boxes, seed0=0):
@@ -48,9 +69,9 @@ def test_ensemble_matches_per_box_solvers(cuda, viscous):
     for _ in range(3):
         ens.step(q)
     edt = ens.last_dt()
-    for b in range(len(BOXES)):
-        assert torch.equal(ens.box_view(q, b), ref[b]), b
-        assert edt[b] == dts[b]
+    for b, (dims, _, _) in enumerate(BOXES):
+        assert _agrees(ens.box_view(q, b), ref[b], dims), b
+        assert edt[b] == dts[b] if min(dims) > 64 else abs(edt[b] - dts[b]) <= 1e-13 * dts[b]
     ens.close()
 
 
@@ -62,13 +83,17 @@ def test_ensemble_tunings_bit_identical(cuda, tuning):
     import compact_schemes_b200 as cs
     ens = cs.Ensemble(cs.ensemble_tgv(BOXES))
     q = _state(ens, BOXES, 7)
+    q_default = q.clone()
     ref, _ = _per_box(BOXES, q, ens, 2)
+    for _ in range(2):
+        ens.step(q_default)
     ens.set_tuning(**tuning)
     for _ in range(2):
         ens.step(q)
     ens.last_dt()
-    for b in range(len(BOXES)):
-        assert torch.equal(ens.box_view(q, b), ref[b]), b
+    assert torch.equal(q, q_default)
+    for b, (dims, _, _) in enumerate(BOXES):
+        assert _agrees(ens.box_view(q, b), ref[b], dims), b
     ens.close()
 
 
@@ -84,8 +109,8 @@ def test_ensemble_physical_closures(cuda):
     for _ in range(2):
         ens.step(q)
     ens.last_dt()
-    for b in range(len(boxes)):
-        assert torch.equal(ens.box_view(q, b), ref[b]), b
+    for b, (dims, _, _) in enumerate(boxes):
+        assert _agrees(ens.box_view(q, b), ref[b], dims), b
 
 
 def test_ensemble_box_against_oracle(cuda):
@@ -117,8 +142,8 @@ def test_ensemble_autotune_keeps_state(cuda):
     ref, _ = _per_box(BOXES, q, ens, 1)
     ens.step(q)
     ens.last_dt()
-    for b in range(len(BOXES)):
-        assert torch.equal(ens.box_view(q, b), ref[b]), b
+    for b, (dims, _, _) in enumerate(BOXES):
+        assert _agrees(ens.box_view(q, b), ref[b], dims), b
 
 
 def test_ensemble_rejects_unsupported(cuda):
@@ -150,7 +175,8 @@ def test_dependency_wait_timeout_returns_error_and_recovers(cuda):
     ref, dts = _per_box(boxes, q, ens, 2)
     for _ in range(2):
         ens.step(q)
-    assert ens.last_dt() == dts
-    for b in range(len(boxes)):
-        assert torch.equal(ens.box_view(q, b), ref[b]), b
+    edt = ens.last_dt()
+    for b, (dims, _, _) in enumerate(boxes):
+        assert abs(edt[b] - dts[b]) <= 1e-13 * dts[b]
+        assert _agrees(ens.box_view(q, b), ref[b], dims), b
     ens.close()
