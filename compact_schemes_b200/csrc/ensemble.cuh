@@ -86,8 +86,15 @@ static __constant__ EnsBox c_ens_boxes[kEnsMaxBoxes];
 static __constant__ Coeffs c_ens_cf;
 
 // Points per read-modify-write chunk in the ensemble's flux items (fewer than
-// the per-box passes: the items have fewer registers to spare).
-constexpr int kEnsRmwChunk = 2, kEnsRmwChunkRk = 1;
+// the per-box passes: the items have fewer registers to spare; measured on
+// the 64-box set, one point beats two or four).
+#ifndef CSB_ENS_RMW
+#define CSB_ENS_RMW 1
+#endif
+#ifndef CSB_ENS_RMW_RK
+#define CSB_ENS_RMW_RK 1
+#endif
+constexpr int kEnsRmwChunk = CSB_ENS_RMW, kEnsRmwChunkRk = CSB_ENS_RMW_RK;
 
 // Line solves of the work items: fields per warp solve for lines of up to 128
 // points (LT <= 4), and whether the periodic closure rows are formed
