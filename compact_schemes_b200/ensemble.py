@@ -4,8 +4,9 @@ Each box is a SolverConfig (FP64, uniform grid, no GCBC); all boxes share one
 packed device state in which box b's q [5][lmx_b] starts at box_offset(b).  A
 step advances every box by one RK step with its own CFL time step, in one
 persistent launch per RK stage replayed as a captured CUDA graph.  Per box
-the arithmetic is that of Solver.step, so results match a per-box Solver bit
-for bit.
+the arithmetic is that of Solver.step: boxes whose axes all exceed 64 points
+match a per-box Solver bit for bit, shorter axes (solved in 4-point chunks)
+agree with it to rounding.
 """
 from __future__ import annotations
 

@@ -371,8 +371,11 @@ int cs_tgv_init(double *q, int lxi, int let, int lze, double mach, double noise_
  * stage pulls tiles of lines of all boxes from a device work queue ordered so
  * that each box's gradient, x-, y- and z-flux phases follow the phase they
  * depend on; a step (4 stages) replays one captured CUDA graph.  Per box the
- * arithmetic is that of cs_solver_step with a CFL time step, so every box's
- * result is bit-identical to stepping it with its own cs_solver.
+ * arithmetic is that of cs_solver_step with a CFL time step: a box whose axes
+ * all have more than 64 points gives bit for bit the result of its own
+ * cs_solver; lines of up to 64 points are solved in 4-point chunks (two
+ * fields per half-warp) where cs_solver uses 2-point chunks, which agrees
+ * with it to rounding (1e-12 relative per field).
  * The state of all boxes is one packed device array: box b's q [5][lmx_b]
  * starts at cs_ensemble_box_offset(b).  At most 96 boxes per ensemble; the
  * stage kernel reads the box table from constant memory that every ensemble
