@@ -129,6 +129,30 @@ def test_ensemble_box_against_oracle(cuda):
     assert err < 1e-12
 
 
+@pytest.mark.parametrize("nbc_code", [45, 10])
+def test_ensemble_ragged_short_lines_against_oracle(cuda, nbc_code):
+    """Axes of up to 64 points that are not multiples of the 4-point chunk
+    (last chunk of 2 or 3 points, 7 to 13 chunks): the half-warp solves of the
+    ensemble against the FP64 oracle, periodic (45) and physical (10) closures."""
+    import compact_schemes_b200 as cs
+    boxes = [((50, 36, 27), 0.1, 1200.0), ((27, 62, 44), 0.2, 900.0)]
+    nbc = [[nbc_code] * 3] * 2
+    ens = cs.Ensemble([cs.tgv_config(None, mach=m, re=r, dims=d, nbc=nbc) for d, m, r in boxes])
+    q = _state(ens, boxes, 13)
+    qo = [ens.box_view(q, b).cpu().numpy().copy() for b in range(len(boxes))]
+    ens.step(q)
+    ens.last_dt()
+    for b, (dims, mach, re) in enumerate(boxes):
+        O.rk_step(qo[b], mach / re, O.uniform_metrics(*dims), dims, nbc, cfl=0.5)
+        got = ens.box_view(q, b).cpu().numpy().reshape(5, -1)
+        ref = qo[b].reshape(5, -1)
+        mom = max(np.abs(ref[m]).max() for m in (1, 2, 3))
+        err = max(np.abs(got[m] - ref[m]).max() / (mom if m in (1, 2, 3) else np.abs(ref[m]).max())
+                  for m in range(5))
+        assert err < 1e-12, (dims, err)
+    ens.close()
+
+
 def test_ensemble_autotune_keeps_state(cuda):
     import torch
     import compact_schemes_b200 as cs
